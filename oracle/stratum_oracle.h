@@ -1,0 +1,72 @@
+/* Test infrastructure only: the CPU oracle (a restatement of the reference's
+ * frame path) used by tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg.  The product never links it.
+ *
+ * Buffer layouts are those of the reference entry points:
+ *   World   16,384 x 16 f32   [w,d,h,type,mat,floors,seed,storey,roofScale,turn,ox,oz,palette,-,-,valid]
+ *   Tags    16,384 x 4  u32   64-bit lot address (xl,xh,zl,zh)
+ *   Nodes   16,384 x 128 x 8 f32   node = [lo.xyz, count, hi.xyz, group]
+ *   Hit     P x 4 f32  [t, fid, material, seed];  Surface P x 4 f32 [n.xyz, slot]
+ *   Linear, History  P x 4 f32;  Pixels P u32 (RGBA8)
+ * Feature record (test interface): 10 f32 [p.xyz, h.xyz, shape, material, turn, seed].
+ */
+#ifndef STRATUM_ORACLE_H
+#define STRATUM_ORACLE_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Work counters filled by orc_trace / orc_shade (indices). */
+enum {
+  ORC_RAYS = 0,      /* primary rays traced */
+  ORC_DDA = 1,       /* lot DDA cells visited (trace.cu:47) */
+  ORC_NODE = 2,      /* nodeNear tests (trace.cu:2) */
+  ORC_GROUP = 3,     /* mode-0 group emissions (trace.cu:22) */
+  ORC_FEAT = 4,      /* featureHit calls (sink.cu:22) */
+  ORC_FOLIAGE = 5,   /* foliage DDA cells (geometry.cu:17) */
+  ORC_MASONRY = 6,   /* masonry relief iterations (geometry.cu:87) */
+  ORC_SDDA = 7,      /* shadow DDA cells (shade.cu:9) */
+  ORC_SHADED = 8,    /* hit pixels shaded (not sky) */
+  ORC_COUNTERS = 16
+};
+
+void orc_offset_tag(const uint32_t* origin, int dx, int dz, uint32_t* out4);
+uint32_t orc_tag_hash(const uint32_t* tag4, int seed);
+uint32_t orc_hashU(uint32_t x);
+void orc_describe_lot(const uint32_t* tag4, int seed, float* out16);
+
+void orc_initCamera(float* C, uint32_t* Origin, int seed);
+void orc_stepCamera(float* C, uint32_t* Origin, const float* I, float dt, int width, int height);
+void orc_clearQueue(uint32_t* Queue);
+void orc_prepareLots(const uint32_t* Origin, const float* C, float* World, uint32_t* Tags, uint32_t* Queue);
+void orc_planBounds(const uint32_t* Queue, uint32_t* Args);
+void orc_buildBounds(const uint32_t* Queue, const float* World, float* Nodes, int nthreads);
+
+int orc_enumerate(const float* lot16, int group, float* out10, int cap);
+void orc_group_bounds(const float* lot16, int group, float* out7);
+float orc_featureHit(const float* f10, const float* ro, const float* rd, float cone);
+void orc_featureNormal(const float* f10, const float* point, float* n3);
+double orc_featureHit_f64(const float* f10, const double* ro, const double* rd, double cone);
+void orc_featureNormal_f64(const float* f10, const double* point, double* n3);
+float orc_queryLot(const float* lot16, const float* nodes128, const float* ro, const float* rd, float best,
+                   float cone, int* fid, float* f10);
+float orc_queryLot_exhaustive(const float* lot16, const float* ro, const float* rd, float best, float cone,
+                              int* fid, float* f10);
+
+/* second (may be NULL): per pixel, the second-smallest candidate distance seen
+ * by the ray (FAR if none) -- the tie rule for identity comparisons. */
+void orc_tracePrimary(const float* World, const float* Nodes, const uint32_t* Origin, const float* C, float* Hit,
+                      float* Surface, int width, int height, int rowStart, int rowCount, int nthreads,
+                      int64_t* counters, float* second);
+void orc_shadePixels(const float* World, const uint32_t* Origin, const float* C, const float* Hit,
+                     const float* Surface, float* Linear, int width, int height, int rowStart, int rowCount,
+                     int nthreads, int64_t* counters);
+void orc_resolveFrame(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
+                      const float* Surface, int width, int height, int nthreads);
+void orc_probeGrammar(const float* Inputs, float* Output);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
