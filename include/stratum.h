@@ -1,0 +1,140 @@
+/* stratum.h -- C ABI of the B200 STRATUM frame path.
+ *
+ * Drop-in for the reference's frame path (stratum-hyperdetail, kernels/*.cu,
+ * driven by src/engine.js).  Each reference __global__ entry point becomes one
+ * function taking exactly the reference's device buffers and scalars, plus a
+ * CUDA stream.  Buffers are owned by the caller and live in device memory;
+ * layouts are the reference's (src/engine.js:41-42,58):
+ *
+ *   World    16,384 x 16 f32   per slot [w,d,h,type,mat,floors,seed,storey,roofScale,
+ *                               turn,ox,oz,palette,-,-,valid]  (kernels/world.cu:100-102)
+ *   Tags     16,384 x 4 u32    64-bit lot address per slot (xl,xh,zl,zh)
+ *   Nodes    16,384 x 128 x 8 f32 = 64 MiB   node = [lo.xyz, count, hi.xyz, group]
+ *   Origin   4 u32              64-bit table origin (xl,xh,zl,zh)
+ *   C        64 f32             camera/view state (field map in kernels/world.cu:57-91)
+ *   I        32 f32             input state (src/app.js:48-57)
+ *   Queue    1 + 16,384 u32     refresh count + queued slots
+ *   Args     8 x 21 u32         per-chunk dispatch sizes
+ *   Hit      W*H x 4 f32        [t, fid, material, seed]; fid -10000 = sky, -1 = ground
+ *   Surface  W*H x 4 f32        [n.xyz, slot]
+ *   Linear, History  W*H x 4 f32;   Pixels  W*H u32 (RGBA8)
+ *
+ * Every function returns STRATUM_OK (0) after enqueueing its work on `stream`,
+ * STRATUM_EINVAL for a bad argument (nothing is launched), or -(cudaError_t)
+ * when the launch itself failed.  Positive values are service statuses.
+ * Nothing here allocates or synchronises unless stated.
+ */
+#ifndef STRATUM_H
+#define STRATUM_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* stratum_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+#define STRATUM_OK 0
+#define STRATUM_EINVAL (-100000)
+#define STRATUM_QUEUE_STALLED 1      /* a bounded device wait ran out */
+#define STRATUM_BUDGET_EXCEEDED 2    /* admission refused: HBM budget */
+#define STRATUM_NOT_FOUND 3          /* unknown session / request */
+
+/* ABI constants (kernels/common.cu:2-16 == src/engine.js:2) */
+#define STRATUM_WORLD_SIDE 128
+#define STRATUM_WORLD_LOTS 16384
+#define STRATUM_LOT_FLOATS 16
+#define STRATUM_CLUSTERS 64
+#define STRATUM_GROUP_NODES 128
+#define STRATUM_MAX_FEATURES 64
+#define STRATUM_BUILD_CHUNK 2048
+#define STRATUM_BUILD_CHUNKS 8
+#define STRATUM_RAY_DISTANCE 2000
+#define STRATUM_MAX_DIM 16384
+
+/* ---- camera and world (kernels/world.cu) ---------------------------------- */
+/* initCamera(float*C, unsigned*Origin, int seed)          kernels/world.cu:57 */
+int stratum_initCamera(float* C, unsigned* Origin, int seed, stratum_stream_t stream);
+/* stepCamera(C, Origin, I, dt, width, height)              kernels/world.cu:64 */
+int stratum_stepCamera(float* C, unsigned* Origin, const float* I, float dt, int width, int height,
+                       stratum_stream_t stream);
+/* clearQueue(unsigned*Queue)                               kernels/world.cu:93 */
+int stratum_clearQueue(unsigned* Queue, stratum_stream_t stream);
+/* prepareLots(Origin, C, World, Tags, Queue)               kernels/world.cu:94
+ * Queue order follows device atomics (varies run to run); its set does not. */
+int stratum_prepareLots(const unsigned* Origin, const float* C, float* World, unsigned* Tags, unsigned* Queue,
+                        stratum_stream_t stream);
+/* planBounds(Queue, Args)                                  kernels/world.cu:106 */
+int stratum_planBounds(const unsigned* Queue, unsigned* Args, stratum_stream_t stream);
+
+/* ---- bounding hierarchy (kernels/accel.cu) -------------------------------- */
+/* buildGroupBounds(Queue, World, Nodes, queueBase)         kernels/accel.cu:2
+ * Lots queueBase .. queueBase+2047 of the queue (the reference's indirect
+ * dispatch becomes a fixed grid whose surplus blocks exit). */
+int stratum_buildGroupBounds(const unsigned* Queue, const float* World, float* Nodes, int queueBase,
+                             stratum_stream_t stream);
+/* reduceGroupBounds(Queue, Nodes, first, queueBase)         kernels/accel.cu:9
+ * first in {32,16,8,4,2,1}. */
+int stratum_reduceGroupBounds(const unsigned* Queue, float* Nodes, int first, int queueBase, stratum_stream_t stream);
+
+/* ---- frame (kernels/trace.cu, kernels/shade.cu) --------------------------- */
+/* tracePrimary(World, Nodes, Origin, C, Hit, Surface, width, height, rowStart, rowCount)   kernels/trace.cu:29 */
+int stratum_tracePrimary(const float* World, const float* Nodes, const unsigned* Origin, const float* C, float* Hit,
+                         float* Surface, int width, int height, int rowStart, int rowCount, stratum_stream_t stream);
+/* shadePixels(World, Origin, C, Hit, Surface, Linear, width, height, rowStart, rowCount)    kernels/shade.cu:45 */
+int stratum_shadePixels(const float* World, const unsigned* Origin, const float* C, const float* Hit,
+                        const float* Surface, float* Linear, int width, int height, int rowStart, int rowCount,
+                        stratum_stream_t stream);
+/* resolveFrame(Linear, History, Pixels, C, Hit, Surface, width, height)                     kernels/shade.cu:104 */
+int stratum_resolveFrame(const float* Linear, float* History, unsigned* Pixels, const float* C, const float* Hit,
+                         const float* Surface, int width, int height, stratum_stream_t stream);
+/* probeGrammar(Inputs[17], Output[16])                      kernels/probe.cu:2 */
+int stratum_probeGrammar(const float* Inputs, float* Output, stratum_stream_t stream);
+
+/* ---- north_star names of the same roles (legacy names of Stratum.cu) ------ */
+/* initWorld = initCamera (Stratum.cu:95 role)                                   */
+int stratum_initWorld(float* C, unsigned* Origin, int seed, stratum_stream_t stream);
+/* schedulePages = clearQueue + prepareLots (Stratum.cu:172 role)                */
+int stratum_schedulePages(const unsigned* Origin, const float* C, float* World, unsigned* Tags, unsigned* Queue,
+                          stratum_stream_t stream);
+/* commitPages = planBounds (Stratum.cu:186 role)                                */
+int stratum_commitPages(const unsigned* Queue, unsigned* Args, stratum_stream_t stream);
+/* buildBVH = buildGroupBounds + reduceGroupBounds x6 over the whole queue, as
+ * one fused kernel (a block per lot; same bits).  Replaces the 8 x 7 indirect
+ * dispatches of src/engine.js:71,74. */
+int stratum_buildBVH(const unsigned* Queue, const float* World, float* Nodes, stratum_stream_t stream);
+
+/* ---- whole frame (the ordered sequence of src/engine.js:67-83) ------------ */
+/* stepCamera, clearQueue, prepareLots, planBounds, buildBVH, then trace and
+ * shade in 64-row strips and resolveFrame.  `Args` may be NULL. */
+int stratum_frame(float* C, unsigned* Origin, const float* I, float dt, float* World, unsigned* Tags, float* Nodes,
+                  unsigned* Queue, unsigned* Args, float* Hit, float* Surface, float* Linear, float* History,
+                  unsigned* Pixels, int width, int height, int draw, stratum_stream_t stream);
+
+/* ---- grammar services (test and tooling) ---------------------------------- */
+/* Feature records of `pairs` (lot, group) pairs: Lots = pairs x 16 f32 World
+ * rows, Groups = pairs i32.  Records = pairs x cap x 10 f32
+ * [p.xyz, h.xyz, shape, material, turn, seed]; Counts = pairs i32 (full count,
+ * even when above cap).  cap <= 64. */
+int stratum_enumerateGroups(const float* Lots, const int* Groups, int pairs, int cap, float* Records, int* Counts,
+                            stratum_stream_t stream);
+/* Analytic test of n (feature, ray) rows [feature(10), ro(3), rd(3), cone] ->
+ * Results n x [t, normal.xyz] (kernels/geometry.cu:33,92). */
+int stratum_featureQuery(const float* Queries, int n, float* Results, stratum_stream_t stream);
+
+/* ---- batched views --------------------------------------------------------- */
+/* Per-view state packed view after view: C v*64, Origin v*4, I v*32, dt v,
+ * wh 2*v (width, height), World v*16384*16, Tags v*16384*4, Queue v*16385,
+ * Nodes v*16384*128*8. */
+int stratum_stepCameras(float* C, unsigned* Origin, const float* I, const float* dt, const int* wh, int views,
+                        stratum_stream_t stream);
+int stratum_prepareLotsBatch(const unsigned* Origin, const float* C, float* World, unsigned* Tags, unsigned* Queue,
+                             int views, stratum_stream_t stream);
+/* All views' lot refreshes in one fused build launch. */
+int stratum_buildBVHBatch(const unsigned* Queue, const float* World, float* Nodes, int views, stratum_stream_t stream);
+
+/* Library version string. */
+const char* stratum_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STRATUM_H */

@@ -1,0 +1,70 @@
+"""The C-ABI library loads and exports exactly what include/stratum.h declares.
+
+No compute calls: this runs without a GPU.  Argument checks that return before
+any CUDA call are exercised (they must not touch the device).
+"""
+import ctypes as ct
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    text = (ROOT / "include" / "stratum.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(stratum_\w+)\s*\(", text)))
+
+
+def test_header_declares_reference_entry_points():
+    names = declared_symbols()
+    for ref_name in ("initCamera", "stepCamera", "clearQueue", "prepareLots", "planBounds", "buildGroupBounds",
+                     "reduceGroupBounds", "tracePrimary", "shadePixels", "resolveFrame", "probeGrammar"):
+        assert f"stratum_{ref_name}" in names
+    for alias in ("initWorld", "schedulePages", "commitPages", "buildBVH", "frame"):
+        assert f"stratum_{alias}" in names
+
+
+def test_library_exports_every_declared_symbol():
+    import stratum_hyperdetail_b200 as sb
+    L = sb.lib()
+    missing = [n for n in declared_symbols() if not hasattr(L, n)]
+    assert not missing, missing
+    assert b"sm_100a" in L.stratum_version()
+
+
+def test_python_signatures_cover_header():
+    import stratum_hyperdetail_b200 as sb
+    assert set(declared_symbols()) - {"stratum_version"} <= set(sb.SIGNATURES)
+
+
+def test_bad_arguments_are_rejected_before_launch():
+    import stratum_hyperdetail_b200 as sb
+    L = sb.lib()
+    assert L.stratum_initCamera(None, None, 1, None) == sb.EINVAL
+    assert L.stratum_tracePrimary(None, None, None, None, None, None, 320, 180, 0, 64, None) == sb.EINVAL
+    assert L.stratum_reduceGroupBounds(ct.c_void_p(16), ct.c_void_p(16), 3, 0, None) == sb.EINVAL
+    assert L.stratum_resolveFrame(None, None, None, None, None, None, -1, 5, None) == sb.EINVAL
+    assert L.stratum_enumerateGroups(None, None, 1, 65, None, None, None) == sb.EINVAL
+
+
+def test_abi_constants_match_reference():
+    # kernels/common.cu:2-16 == src/engine.js:2 of the reference
+    text = (ROOT / "include" / "stratum.h").read_text()
+    want = {"WORLD_SIDE": 128, "WORLD_LOTS": 16384, "LOT_FLOATS": 16, "CLUSTERS": 64, "GROUP_NODES": 128,
+            "MAX_FEATURES": 64, "BUILD_CHUNK": 2048, "BUILD_CHUNKS": 8, "RAY_DISTANCE": 2000}
+    for k, v in want.items():
+        assert re.search(rf"#define STRATUM_{k} {v}\b", text), k
+    assert want["GROUP_NODES"] == 2 * want["CLUSTERS"]
+    assert want["RAY_DISTANCE"] < (want["WORLD_SIDE"] / 2 - 2) * 36
+
+
+def test_engine_fails_loudly_without_gpu():
+    import torch
+    import stratum_hyperdetail_b200 as sb
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(RuntimeError):
+        sb.Engine().init(320, 180)

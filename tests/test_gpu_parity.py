@@ -1,0 +1,168 @@
+"""CUDA path vs the CPU oracle, through the C ABI, on the same seeded inputs.
+
+Bit-exact: 64-bit addressing, lot descriptors, refresh queue (as a set),
+indirect args, feature records, group bounds and the whole hierarchy.
+Tolerance (stated by the frame-path spec): hit identity must match on every
+ray whose two nearest candidates differ by more than the distance tolerance;
+hit distance and normal within 1e-5 relative; linear colour within 1/1024
+per channel, with mismatches counted and reported.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import oracle_lib as ol
+from gpu_lib import Frame, GpuWorld, compare_frames, s, setup_pose, u32
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TOL_T, TOL_N, TOL_C = 1e-5, 1e-5, 1.0 / 1024.0
+POSES = {  # name -> (pos, yaw, pitch, w, h)
+    "config1": ((32.0, 1.7, 32.0), np.pi / 4, 0.0, 320, 180),
+    "street": ((14.0, 1.7, 14.0), 0.0, 0.0, 160, 90),
+    "rooftop": ((14.0, 40.0, 14.0), np.pi / 2, 0.0, 160, 90),
+    "aerial": ((14.0, 300.0, 14.0), 0.6, -np.pi / 6, 160, 90),
+}
+
+
+def test_probe_fixtures(cuda, oracle):
+    from stratum_hyperdetail_b200 import call, ptr
+    fixtures = json.loads((GOLDEN / "probes.json").read_text())
+    for f in fixtures:
+        inp = torch.tensor(f["input"], dtype=torch.float32, device="cuda")
+        out = torch.zeros(16, dtype=torch.float32, device="cuda")
+        call("stratum_probeGrammar", ptr(inp), ptr(out), s())
+        got = out.cpu().numpy()
+        want = oracle.probe(np.array(f["input"], np.float32))
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), (f["input"], got, want)
+        assert np.allclose(got, f["expected"], rtol=1e-5, atol=1e-4)
+
+
+def test_enumeration_records_bit_exact(cuda, oracle):
+    from stratum_hyperdetail_b200 import call, ptr
+    rng = np.random.default_rng(3)
+    lots, groups = [], []
+    for i in range(48):
+        tag = rng.integers(0, 2**32, 4, dtype=np.uint64).astype(np.uint32)
+        lot = oracle.describe_lot(tag, int(rng.integers(0, 30000)))
+        lot[3] = i % 6
+        for g in range(64):
+            lots.append(lot)
+            groups.append(g)
+    L = torch.from_numpy(np.array(lots, np.float32)).cuda()
+    G = torch.tensor(groups, dtype=torch.int32, device="cuda")
+    n = len(groups)
+    rec = torch.zeros(n * 64 * 10, dtype=torch.float32, device="cuda")
+    cnt = torch.zeros(n, dtype=torch.int32, device="cuda")
+    call("stratum_enumerateGroups", ptr(L), ptr(G), n, 64, ptr(rec), ptr(cnt), s())
+    rec = rec.cpu().numpy().reshape(n, 64, 10)
+    cnt = cnt.cpu().numpy()
+    total = 0
+    for i in range(n):
+        want = oracle.enumerate(lots[i], groups[i])
+        assert cnt[i] == len(want), (i, groups[i])
+        assert np.array_equal(rec[i, :cnt[i]].view(np.uint32), want.view(np.uint32)), (i, groups[i])
+        total += cnt[i]
+    assert total > 50000
+
+
+def test_feature_query_vs_oracle_and_fp64(cuda, oracle):
+    """featureHit/featureNormal on the GPU == oracle, and within 1e-5 of an FP64 re-intersection."""
+    from stratum_hyperdetail_b200 import call, ptr
+    rng = np.random.default_rng(9)
+    lot = oracle.describe_lot(np.array([3, 0, 9, 0], np.uint32), 1788)
+    feats = []
+    for ty in range(5):
+        l2 = lot.copy()
+        l2[3] = ty
+        for g in range(64):
+            feats.extend(oracle.enumerate(l2, g))
+    feats = np.array(feats, np.float32)
+    rows = []
+    for i in rng.choice(len(feats), 2000, replace=False):
+        f = feats[i]
+        ro = (f[:3] + rng.normal(0, 5, 3)).astype(np.float32)
+        rd = (f[:3] + rng.normal(0, 0.3, 3) - ro).astype(np.float32)
+        rd /= np.float32(np.linalg.norm(rd))
+        rows.append(np.concatenate([f, ro, rd, [0.0]]).astype(np.float32))
+    q = np.array(rows, np.float32)
+    Q = torch.from_numpy(q).cuda()
+    R = torch.zeros(len(q) * 4, dtype=torch.float32, device="cuda")
+    call("stratum_featureQuery", ptr(Q), len(q), ptr(R), s())
+    r = R.cpu().numpy().reshape(-1, 4)
+    hits = fp64_bad = 0
+    for i, row in enumerate(q):
+        f, ro, rd = row[:10], row[10:13], row[13:16]
+        t = oracle.feature_hit(f, ro, rd, 0.0)
+        assert np.float32(t).view(np.uint32) == r[i, 0].view(np.uint32), (i, t, r[i, 0])
+        if t < 2000:
+            hits += 1
+            # FP64 re-intersection of the same feature with the same (float) ray
+            t64 = oracle.feature_hit_f64(f, ro.astype(np.float64), rd.astype(np.float64), 0.0)
+            if f[6] == 1 and f[7] == 7:
+                continue  # leaf discs: a DDA whose cell sequence may legitimately differ in FP64
+            if abs(t64 - r[i, 0]) > TOL_T * max(t64, 1e-3):
+                fp64_bad += 1
+    assert hits > 300
+    assert fp64_bad <= len(q) * 0.002, fp64_bad
+
+
+@pytest.mark.parametrize("name", list(POSES))
+def test_table_and_hierarchy_bit_exact(cuda, oracle, name):
+    pos, yaw, pitch, w, h = POSES[name]
+    g = setup_pose(0x5EED, pos, yaw, pitch, w, h)
+    o = ol.setup_pose(oracle, 0x5EED, pos, yaw, pitch, w, h)
+    assert np.array_equal(g.C.cpu().numpy().view(np.uint32), o.C.view(np.uint32))
+    assert np.array_equal(u32(g.Origin), o.Origin)
+    assert np.array_equal(g.World.cpu().numpy().view(np.uint32), o.World.view(np.uint32))
+    assert np.array_equal(u32(g.Tags), o.Tags)
+    gq = u32(g.Queue)
+    assert gq[0] == o.Queue[0] == 16384
+    assert np.array_equal(np.sort(gq[1:gq[0] + 1]), np.sort(o.Queue[1:o.Queue[0] + 1]))
+    assert np.array_equal(u32(g.Args), o.Args)
+    assert np.array_equal(g.Nodes.cpu().numpy(), o.Nodes)
+
+
+def test_drop_in_chunked_build_equals_fused(cuda, oracle):
+    pos, yaw, pitch, w, h = POSES["config1"]
+    a = setup_pose(0x5EED, pos, yaw, pitch, w, h, drop_in=True)
+    b = setup_pose(0x5EED, pos, yaw, pitch, w, h, drop_in=False)
+    assert np.array_equal(a.Nodes.cpu().numpy(), b.Nodes.cpu().numpy())
+
+
+@pytest.mark.parametrize("name", list(POSES))
+def test_frame_parity(cuda, oracle, name):
+    pos, yaw, pitch, w, h = POSES[name]
+    g = setup_pose(0x5EED, pos, yaw, pitch, w, h)
+    fr = Frame(w, h).render(g)
+    o = ol.setup_pose(oracle, 0x5EED, pos, yaw, pitch, w, h)
+    second = np.zeros(w * h, np.float32)
+    orc = ol.render(oracle, o, w, h, second=second)
+    rep = compare_frames(fr, orc, second, TOL_T, TOL_N, TOL_C)
+    print(name, rep)
+    assert rep["identity_bad"] == 0, rep
+    assert rep["t_bad"] == 0 and rep["n_bad"] == 0 and rep["material_bad"] == 0, rep
+    # colour: mismatches are counted; allow a tiny fraction at texture discontinuities
+    assert rep["linear_bad"] <= max(2, rep["rays"] // 2000), rep
+    assert rep["history_bad"] <= max(2, rep["rays"] // 2000), rep
+
+
+def test_sample_accumulation_converges(cuda, oracle):
+    """64-sample stationary accumulation: C[19] reaches 64, History count 64, then frozen."""
+    from stratum_hyperdetail_b200 import call, ptr
+    pos, yaw, pitch, w, h = POSES["street"]
+    g = setup_pose(0x5EED, pos, yaw, pitch, w, h)
+    fr = Frame(w, h)
+    for i in range(66):
+        call("stratum_stepCamera", ptr(g.C), ptr(g.Origin), ptr(g.I), 0.0, w, h, s())
+        fr.render(g)
+    assert g.C[19].item() == 64.0
+    hist = fr.History.cpu().numpy().reshape(-1, 4)
+    assert np.all(hist[:, 3] == 64.0)
+    before = fr.History.clone()
+    call("stratum_stepCamera", ptr(g.C), ptr(g.Origin), ptr(g.I), 0.0, w, h, s())
+    fr.render(g)
+    assert torch.equal(before, fr.History)
