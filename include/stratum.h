@@ -131,6 +131,13 @@ int stratum_prepareLotsBatch(const unsigned* Origin, const float* C, float* Worl
 /* All views' lot refreshes in one fused build launch. */
 int stratum_buildBVHBatch(const unsigned* Queue, const float* World, float* Nodes, int views, stratum_stream_t stream);
 
+/* ---- measurement ------------------------------------------------------------ */
+/* FP32 issue-rate probe: `blocks` x 256 threads, each `iters` iterations of 8
+ * independent multiply-add chains (2 ops each).  Lane ops per launch =
+ * blocks * 256 * iters * 16.  Used as the roofline denominator of the frame
+ * path (its kernels are FP32-issue bound).  `out` receives nothing in practice. */
+int stratum_issueProbe(float* out, int blocks, int iters, stratum_stream_t stream);
+
 /* Library version string. */
 const char* stratum_version(void);
 

@@ -147,6 +147,17 @@ void ref_resolveFrame(const float* Linear, float* History, unsigned* Pixels, con
       resolveFrame(Linear, History, Pixels, C, Hit, Surface, width, height);
     }
 }
+// resolveFrame over rows [rowStart, rowStart+rowCount) only (timing samples).
+void ref_resolveRows(const float* Linear, float* History, unsigned* Pixels, const float* C, const float* Hit,
+                     const float* Surface, int width, int height, int rowStart, int rowCount, int nthreads) {
+  const int yEnd = rowStart + rowCount < height ? rowStart + rowCount : height;
+#pragma omp parallel for schedule(dynamic, 4) num_threads(threads(nthreads))
+  for (int y = rowStart; y < yEnd; y++)
+    for (int x = 0; x < width; x++) {
+      set_pixel(x, y);
+      resolveFrame(Linear, History, Pixels, C, Hit, Surface, width, height);
+    }
+}
 void ref_probeGrammar(const float* Inputs, float* Output) { one_thread(); probeGrammar(Inputs, Output); }
 
 // Feature records of one group: 10 floats each [p.xyz, h.xyz, shape, material,

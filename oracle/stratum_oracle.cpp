@@ -306,6 +306,8 @@ template <class R> R hitFeature(const Feat& f, V3<R> ro, V3<R> rd, R cone, Count
   Span<R> range = slab(p, d, h * R(-1), h);
   if (shape == 3 || shape == 4) range = slab(p, d, mk(-h.x, R(0), -h.z), h);
   if (range.hi < std::fmax(R(0.001f), range.lo)) return R(kFar);
+  if (cn) cn->v[shape == 0 ? ORC_PASS_BOX : shape == 1 ? ORC_PASS_ELLIPSOID : shape == 2 ? ORC_PASS_CYLINDER
+                : shape == 3 ? ORC_PASS_PRISM : ORC_PASS_ARCH]++;
   R t = range.lo > R(0.001f) ? range.lo : range.hi;
   if (shape == 1) {  // ellipsoid
     V3<R> a = mk(p.x / h.x, p.y / h.y, p.z / h.z), v = mk(d.x / h.x, d.y / h.y, d.z / h.z);
@@ -1096,6 +1098,7 @@ void shadePixel(const float* W, const uint32_t* O, const float* C, const float* 
       mat = std::fabs(q.x) < 16.5f && std::fabs(q.z) < 16.5f ? 11 : 10;
       if (lot.type == 5) mat = 9;
     }
+    if (cn && (mat == 0 || mat == 1)) cn->v[ORC_SHADED_MASONRY]++;
     if (mat == 7 && dot(n, rd) > 0.0f) { n = n * -1.0f; qn = qn * -1.0f; }
     float footprint = std::fmax(0.00005f, t * 1.08f / float(height));
     float sfp = footprint / std::fmax(0.18f, std::fabs(dot(n, rd)));
@@ -1393,6 +1396,13 @@ void orc_resolveFrame(const float* Lin, float* Hist, uint32_t* Px, const float* 
                       int width, int height, int nthreads) {
 #pragma omp parallel for schedule(dynamic, 2) num_threads(useThreads(nthreads))
   for (int y = 0; y < height; y++)
+    for (int x = 0; x < width; x++) resolvePixel(Lin, Hist, Px, C, Hit, Surf, width, height, x, y);
+}
+void orc_resolveRows(const float* Lin, float* Hist, uint32_t* Px, const float* C, const float* Hit, const float* Surf,
+                     int width, int height, int rowStart, int rowCount, int nthreads) {
+  const int yEnd = std::min(height, rowStart + rowCount);
+#pragma omp parallel for schedule(dynamic, 2) num_threads(useThreads(nthreads))
+  for (int y = rowStart; y < yEnd; y++)
     for (int x = 0; x < width; x++) resolvePixel(Lin, Hist, Px, C, Hit, Surf, width, height, x, y);
 }
 // probe.cu:2-14

@@ -28,7 +28,14 @@ enum {
   ORC_MASONRY = 6,   /* masonry relief iterations (geometry.cu:87) */
   ORC_SDDA = 7,      /* shadow DDA cells (shade.cu:9) */
   ORC_SHADED = 8,    /* hit pixels shaded (not sky) */
-  ORC_COUNTERS = 16
+  ORC_SHADED_MASONRY = 9,  /* shaded pixels of brick/stone (materials 0, 1) */
+  ORC_PASS_BOX = 10,       /* featureHit calls past the slab test, by shape */
+  ORC_PASS_ELLIPSOID = 11,
+  ORC_PASS_CYLINDER = 12,
+  ORC_PASS_PRISM = 13,
+  ORC_PASS_ARCH = 14,      /* shapes 4 and 7 */
+  ORC_EMIT = 15,           /* features emitted in mode 0 (same as ORC_FEAT) */
+  ORC_COUNTERS = 32
 };
 
 void orc_offset_tag(const uint32_t* origin, int dx, int dz, uint32_t* out4);
@@ -64,6 +71,8 @@ void orc_shadePixels(const float* World, const uint32_t* Origin, const float* C,
                      int nthreads, int64_t* counters);
 void orc_resolveFrame(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
                       const float* Surface, int width, int height, int nthreads);
+void orc_resolveRows(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
+                     const float* Surface, int width, int height, int rowStart, int rowCount, int nthreads);
 void orc_probeGrammar(const float* Inputs, float* Output);
 
 #ifdef __cplusplus

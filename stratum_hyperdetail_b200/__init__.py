@@ -68,6 +68,7 @@ SIGNATURES: dict[str, list] = {
     "stratum_stepCameras": [_P, _P, _P, _P, _P, _I, _S],
     "stratum_prepareLotsBatch": [_P, _P, _P, _P, _P, _I, _S],
     "stratum_buildBVHBatch": [_P, _P, _P, _I, _S],
+    "stratum_issueProbe": [_P, _I, _I, _S],
 }
 
 _lib = None

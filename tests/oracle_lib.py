@@ -136,6 +136,7 @@ class Oracle(_Lib):
         L.orc_shadePixels.argtypes = [f32p, u32p, f32p, f32p, f32p, f32p, ct.c_int, ct.c_int, ct.c_int, ct.c_int,
                                       ct.c_int, ct.c_void_p]
         L.orc_resolveFrame.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p, ct.c_int, ct.c_int, ct.c_int]
+        L.orc_resolveRows.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p] + [ct.c_int] * 5
         L.orc_featureHit_f64.restype = ct.c_double
         L.orc_featureHit_f64.argtypes = [f32p, f64p, f64p, ct.c_double]
         L.orc_featureNormal_f64.argtypes = [f32p, f64p, f64p]
@@ -159,6 +160,9 @@ class Oracle(_Lib):
 
     def resolve(self, linear, history, pixels, C, hit, surface, w, h, nthreads=0):
         self.lib.orc_resolveFrame(linear, history, pixels, C, hit, surface, w, h, nthreads)
+
+    def resolve_rows(self, linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads=0):
+        self.lib.orc_resolveRows(linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads)
 
     def feature_hit_f64(self, f10, ro, rd, cone=0.0):
         return self.lib.orc_featureHit_f64(np.ascontiguousarray(f10, np.float32), np.ascontiguousarray(ro, np.float64),
@@ -188,6 +192,7 @@ class RefLib(_Lib):
         L.ref_tracePrimary.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p] + [ct.c_int] * 5
         L.ref_shadePixels.argtypes = [f32p, u32p, f32p, f32p, f32p, f32p] + [ct.c_int] * 5
         L.ref_resolveFrame.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p] + [ct.c_int] * 3
+        L.ref_resolveRows.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p] + [ct.c_int] * 5
 
     def build_bounds(self, queue, world, nodes, nthreads=0):
         self.lib.ref_buildBounds(queue, world, nodes, nthreads)
@@ -203,6 +208,9 @@ class RefLib(_Lib):
 
     def resolve(self, linear, history, pixels, C, hit, surface, w, h, nthreads=0):
         self.lib.ref_resolveFrame(linear, history, pixels, C, hit, surface, w, h, nthreads)
+
+    def resolve_rows(self, linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads=0):
+        self.lib.ref_resolveRows(linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads)
 
 
 def ref_available() -> bool:
