@@ -232,93 +232,147 @@ def issue_peak(torch, sb):
     return best
 
 
+def timed_steps(torch, stream, steps, flush, body):
+    """Run `steps` timed steps: L2 flush (untimed), then `body(events)` between
+    two CUDA events on `stream`.  Returns per-step milliseconds and whatever
+    `body` returns per step."""
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    ms, out = [], []
+    for _ in range(steps):
+        flush.zero_()
+        a, b = ev(), ev()
+        a.record(stream)
+        out.append(body())
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    return ms, out
+
+
 def ours_arm(args):
     import torch
     rank, world, local = dist_info()
     dist = init_dist(world)
     torch.cuda.set_device(local)
     import stratum_hyperdetail_b200 as sb
+    from stratum_hyperdetail_b200.batch import Batch
     from stratum_hyperdetail_b200.views import View
     sb.lib()
 
+    names = list(args.poses)
     views = []
-    for name in args.poses:
+    for name in names:
         p = POSES[name]
         v = View(WIDTH, HEIGHT)
         v.set_pose(SEED, p["origin"], p["pos"], p["yaw"], p["pitch"])
-        views.append((name, v))
+        views.append(v)
     torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    rays_per_step = WIDTH * HEIGHT * len(views)
 
-    def step(events=None):
-        n = 0
-        for i, (_, v) in enumerate(views):
-            n += v.frame_parts(0.0, stream, events[i] if events else None)
-        return n
+    # -- 1. the plain per-frame drop-in path (reference launch sequence and shapes)
+    trace_plain = np.zeros(len(views))
+
+    def plain_step():
+        te = [(ev(), ev()) for _ in views]
+        n = sum(v.frame_parts(0.0, stream, te[i]) for i, v in enumerate(views))
+        return n, te
 
     for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    step_ms, trace_ms = [], np.zeros(len(views))
-    launches = 0
-    with ClockSampler(local) as clocks:
-        wall0 = time.perf_counter()
-        for k in range(args.steps):
-            flush.zero_()  # L2 flush, outside the timed step
-            a, b = ev(), ev()
-            te = [(ev(), ev()) for _ in views]
-            a.record(stream)
-            launches += step(te)
-            b.record(stream)
-            b.synchronize()
-            step_ms.append(a.elapsed_time(b))
-            trace_ms += np.array([x.elapsed_time(y) for x, y in te])
+        plain_step()
+    plain_ms, plain_out = timed_steps(torch, stream, args.steps, flush, plain_step)
+    for _, te in plain_out:
+        trace_plain += np.array([x.elapsed_time(y) for x, y in te])
+    plain_value = rays_per_step * args.steps / (sum(plain_ms) * 1e-3)
+    per_pose = {n: WIDTH * HEIGHT * args.steps / (trace_plain[i] * 1e-3) for i, n in enumerate(names)}
+
+    # -- 2. the batched path: every view in one launch per kernel, autotuned
+    batch = Batch(views)
+    batch.frame()
+    tune_ms = batch.autotune()
+    tune = {"threads": batch.tune.threads, "grab": batch.tune.grab, "order": batch.tune.order,
+            "trace_ms": tune_ms}
+    call, P, s = sb.call, sb.ptr, stream.cuda_stream
+
+    def batch_step():
+        t0, t1 = ev(), ev()
+        call("stratum_stepViews", P(batch.table), batch.n, s)
+        batch.refresh(stream)
+        t0.record(stream)
+        batch.trace(stream)
+        t1.record(stream)
+        batch.shade(stream)
+        return t0, t1
+
+    for _ in range(args.warmup):
+        batch_step()
+    eager_ms, eager_out = timed_steps(torch, stream, args.steps, flush, batch_step)
+    trace_batch_ms = sum(a.elapsed_time(b) for a, b in eager_out)
+    eager_value = rays_per_step * args.steps / (sum(eager_ms) * 1e-3)
+
+    # -- 3. the same batched frame captured once as a CUDA graph and replayed (headline)
+    graph_ok = True
+    try:
+        batch.capture()
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        graph_ok = False
+        graph_err = repr(e)
+    if graph_ok:
+        for _ in range(args.warmup):
+            batch.replay()
         torch.cuda.synchronize()
-        wall = time.perf_counter() - wall0
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clocks:
+            wall0 = time.perf_counter()
+            step_ms, _ = timed_steps(torch, stream, args.steps, flush, batch.replay)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - wall0
+        launches = batch.launches_per_frame * args.steps
+        path = "batched: all views per launch, persistent tile queue, CUDA graph replay"
+    else:
+        with ClockSampler(local) as clocks:
+            wall0 = time.perf_counter()
+            step_ms, _ = timed_steps(torch, stream, args.steps, flush, lambda: batch.frame(stream))
+            wall = time.perf_counter() - wall0
+        launches = batch.launches_per_frame * args.steps
+        path = "batched: all views per launch, persistent tile queue (eager; graph capture failed)"
     elapsed = sum(step_ms) * 1e-3
     if dist:
         t = torch.tensor([elapsed], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed = float(t.item())
-    rays_per_step = WIDTH * HEIGHT * len(views)
     value = rays_per_step * args.steps * world / elapsed
-    per_pose = {name: WIDTH * HEIGHT * args.steps / (trace_ms[i] * 1e-3) for i, (name, _) in enumerate(views)}
 
-    # --- roofline of the dominant kernel (tracePrimary): algorithmic FP32 ops / its time
+    # -- roofline of the dominant kernel (traceViewsK): algorithmic FP32 ops / its event time
     peak = issue_peak(torch, sb)
-    trace_ops = sum(OPS_PER_RAY[n][1] for n, _ in views) * WIDTH * HEIGHT * args.steps
-    trace_s = float(trace_ms.sum()) * 1e-3
-    achieved = trace_ops / trace_s
-    launches_trace = args.steps * len(views) * math.ceil(HEIGHT / 64)
-    traffic = (TRACE_DRAM_BYTES_PER_RAY * WIDTH * 64) if TRACE_DRAM_BYTES_PER_RAY else None
+    trace_ops = sum(OPS_PER_RAY[n][1] for n in names) * WIDTH * HEIGHT * args.steps
+    achieved = trace_ops / (trace_batch_ms * 1e-3)
+    traffic = (TRACE_DRAM_BYTES_PER_RAY * rays_per_step) if TRACE_DRAM_BYTES_PER_RAY else None
+    whole_ops = sum(OPS_PER_RAY[n][0] for n in names) * WIDTH * HEIGHT * args.steps
     roofline = {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": "tracePrimaryK",
+                "frac": achieved / peak, "traffic": traffic, "kernel": "traceViewsK (one launch per step)",
                 "peak_source": "measured in this run (stratum_issueProbe: FP32 lane ops/s, no FMA)",
-                "ops_source": "algorithmic FP32 ops per ray from the reference source (oracle/count_work.py)"}
-    whole_ops = sum(OPS_PER_RAY[n][0] for n, _ in views) * WIDTH * HEIGHT * args.steps
-    roofline["path_frac"] = whole_ops / elapsed / world / peak
+                "ops_source": "algorithmic FP32 ops per ray from the reference source (oracle/count_work.py)",
+                "path_frac": whole_ops / elapsed * world / world / peak,
+                "plain_trace_frac": trace_ops / (trace_plain.sum() * 1e-3) / peak}
 
-    # --- e2e through the C-ABI call with host buffers
-    h2d = d2h = 0
+    # -- e2e: the batched C-ABI call with the step's inputs from pinned host memory and RGBA8 back
     host_in = [torch.zeros(32, dtype=torch.float32).pin_memory() for _ in views]
     host_px = [torch.empty(WIDTH * HEIGHT, dtype=torch.int32).pin_memory() for _ in views]
-    e2e_ms = []
-    for k in range(max(2, args.steps // 2) + 1):
-        a, b = ev(), ev()
-        a.record(stream)
-        for i, (_, v) in enumerate(views):
+
+    def e2e_step():
+        for i, v in enumerate(views):
             v.I.copy_(host_in[i], non_blocking=True)
-            v.frame(0.0, stream)
+        batch.frame(stream)
+        for i, v in enumerate(views):
             host_px[i].copy_(v.Pixels, non_blocking=True)
-        b.record(stream)
-        b.synchronize()
-        if k > 0:
-            e2e_ms.append(a.elapsed_time(b))
+
+    e2e_step()
+    e2e_ms, _ = timed_steps(torch, stream, max(3, args.steps // 2), flush, e2e_step)
     h2d = sum(t.numel() * 4 for t in host_in)
     d2h = sum(t.numel() * 4 for t in host_px)
     e2e_value = rays_per_step * len(e2e_ms) * world / (sum(e2e_ms) * 1e-3)
@@ -333,6 +387,8 @@ def ours_arm(args):
 
     if dist:
         dist.barrier()
+    batch.graph = None  # release the graph before the process group
+    if dist:
         dist.destroy_process_group()
     if rank != 0:
         return 0
@@ -342,15 +398,22 @@ def ours_arm(args):
             "data": "synthetic (seeded procedural world, fixed poses)",
             "config": {"workload": "plain single-view frame 1600x900, seed 0x5EED, six poses, one sample per view "
                                    "per step accumulating toward 64",
-                       "width": WIDTH, "height": HEIGHT, "views_per_step": len(views), "poses": POSES,
-                       "path": "plain per-frame drop-in: the reference engine's launch sequence and shapes",
+                       "width": WIDTH, "height": HEIGHT, "views_per_step": len(views),
+                       "poses": {n: POSES[n] for n in names}, "path": path, "tune": tune,
                        "l2": "flushed between timed steps (256 MiB write outside the timed region)",
                        "parallelism": f"replicas x{world}"},
+            "plain_path": {"value": plain_value, "unit": "rays/s", "ms_per_step": sum(plain_ms) / args.steps,
+                           "launches_per_step": plain_out[0][0],
+                           "note": "reference launch structure: per view 15 trace + 15 shade strips of 64 rows"},
+            "batched_eager": {"value": eager_value, "ms_per_step": sum(eager_ms) / args.steps},
+            "batched_vs_plain": value / plain_value,
             "per_pose_trace_rays_per_s": per_pose,
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "call": "stratum_frame per view, pinned host input and RGBA8 readback"},
+                    "call": "stratum_frameViews over the batch, pinned host input and RGBA8 readback"},
             "gpu_launches": launches, "clocks": clocks.summary(), "wall_s": wall}
+    if not graph_ok:
+        line["graph_error"] = graph_err
     print(json.dumps(line), flush=True)
     return 0
 

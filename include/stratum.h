@@ -120,16 +120,66 @@ int stratum_enumerateGroups(const float* Lots, const int* Groups, int pairs, int
  * Results n x [t, normal.xyz] (kernels/geometry.cu:33,92). */
 int stratum_featureQuery(const float* Queries, int n, float* Results, stratum_stream_t stream);
 
-/* ---- batched views --------------------------------------------------------- */
-/* Per-view state packed view after view: C v*64, Origin v*4, I v*32, dt v,
- * wh 2*v (width, height), World v*16384*16, Tags v*16384*4, Queue v*16385,
- * Nodes v*16384*128*8. */
-int stratum_stepCameras(float* C, unsigned* Origin, const float* I, const float* dt, const int* wh, int views,
-                        stratum_stream_t stream);
-int stratum_prepareLotsBatch(const unsigned* Origin, const float* C, float* World, unsigned* Tags, unsigned* Queue,
-                             int views, stratum_stream_t stream);
-/* All views' lot refreshes in one fused build launch. */
-int stratum_buildBVHBatch(const unsigned* Queue, const float* World, float* Nodes, int views, stratum_stream_t stream);
+/* ---- batched views (no reference counterpart: B200 multi-view form) ------- */
+/* One view of a batch: device pointers to that view's own buffers, in the
+ * layouts above, plus its frame size and time step.  A batch is a DEVICE array
+ * of these; tileBase/tilesX are written by stratum_renderViews. */
+typedef struct stratum_view {
+  float* C;
+  unsigned* Origin;
+  const float* I;
+  float* World;
+  unsigned* Tags;
+  float* Nodes;
+  unsigned* Queue;
+  float* Hit;
+  float* Surface;
+  float* Linear;
+  float* History;
+  unsigned* Pixels;
+  int width, height;
+  float dt;
+  int tileBase, tilesX, reserved;
+} stratum_view;
+
+/* Tunables of the batched trace: block size (64/128/256), tiles a warp claims
+ * per queue access (queue depth, 1..16), tile order within a view (0 row-major,
+ * 1 Morton-ordered 4x4-tile super-tiles).  Chosen by stratum_autotune. */
+typedef struct stratum_tune {
+  int threads;
+  int grab;
+  int order;
+} stratum_tune;
+
+/* Device scratch the batched renderer needs for `views` views (work-queue
+ * counters and per-view frame constants).  Zero it once before first use; the
+ * kernels leave their counters at zero when they finish. */
+unsigned long long stratum_batchScratchBytes(int views);
+/* stepCamera of every view (dt from the view). */
+int stratum_stepViews(stratum_view* views, int n, stratum_stream_t stream);
+/* clearQueue + prepareLots of every view, one launch each. */
+int stratum_refreshViews(stratum_view* views, int n, stratum_stream_t stream);
+/* Every view's queued lots rebuilt in one fused launch. */
+int stratum_buildViews(stratum_view* views, int n, stratum_stream_t stream);
+/* All views' primary rays through one persistent kernel pulling 8x4-pixel
+ * tiles from a device work queue, then one persistent shade+resolve pass. */
+int stratum_renderViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                        const stratum_tune* tune, stratum_stream_t stream);
+/* The trace half of renderViews alone (Hit, Surface). */
+int stratum_traceViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                       const stratum_tune* tune, stratum_stream_t stream);
+/* The shade + resolve half alone; follows a traceViews of the same views,
+ * scratch and tune (it reuses that call's tile bases and frame constants). */
+int stratum_shadeViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                       const stratum_tune* tune, stratum_stream_t stream);
+/* Time every candidate tune (block size x queue depth x tile order) on this
+ * batch with CUDA events and return the fastest in *best (and its trace time
+ * in *bestMs when not NULL).  Synchronises `stream`. */
+int stratum_autotune(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes, stratum_tune* best,
+                     float* bestMs, stratum_stream_t stream);
+/* The whole batched frame: stepViews, refreshViews, buildViews, renderViews. */
+int stratum_frameViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                       const stratum_tune* tune, stratum_stream_t stream);
 
 /* ---- measurement ------------------------------------------------------------ */
 /* FP32 issue-rate probe: `blocks` x 256 threads, each `iters` iterations of 8

@@ -65,11 +65,29 @@ SIGNATURES: dict[str, list] = {
     "stratum_frame": [_P, _P, _P, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _S],
     "stratum_enumerateGroups": [_P, _P, _I, _I, _P, _P, _S],
     "stratum_featureQuery": [_P, _I, _P, _S],
-    "stratum_stepCameras": [_P, _P, _P, _P, _P, _I, _S],
-    "stratum_prepareLotsBatch": [_P, _P, _P, _P, _P, _I, _S],
-    "stratum_buildBVHBatch": [_P, _P, _P, _I, _S],
+    "stratum_stepViews": [_P, _I, _S],
+    "stratum_refreshViews": [_P, _I, _S],
+    "stratum_buildViews": [_P, _I, _S],
+    "stratum_traceViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
+    "stratum_shadeViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
+    "stratum_renderViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
+    "stratum_frameViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
+    "stratum_autotune": [_P, _I, _P, ct.c_ulonglong, _P, _P, _S],
     "stratum_issueProbe": [_P, _I, _I, _S],
 }
+
+
+class Tune(ct.Structure):
+    """stratum_tune: block size, tiles per queue claim, tile order."""
+    _fields_ = [("threads", ct.c_int), ("grab", ct.c_int), ("order", ct.c_int)]
+
+
+class ViewRecord(ct.Structure):
+    """stratum_view: one view of a batch (device pointers + size)."""
+    _fields_ = [(n, ct.c_void_p) for n in ("C", "Origin", "I", "World", "Tags", "Nodes", "Queue", "Hit", "Surface",
+                                            "Linear", "History", "Pixels")] + [
+        ("width", ct.c_int), ("height", ct.c_int), ("dt", ct.c_float), ("tileBase", ct.c_int), ("tilesX", ct.c_int),
+        ("reserved", ct.c_int)]
 
 _lib = None
 
@@ -87,6 +105,8 @@ def lib() -> ct.CDLL:
             fn.restype = ct.c_int
         L.stratum_version.restype = ct.c_char_p
         L.stratum_version.argtypes = []
+        L.stratum_batchScratchBytes.restype = ct.c_ulonglong
+        L.stratum_batchScratchBytes.argtypes = [ct.c_int]
         _lib = L
     return _lib
 

@@ -1,0 +1,243 @@
+// Batched multi-view frame path: many views of any resolution, pose and world
+// seed per launch.  Each kernel reads a device table of stratum_view; every
+// per-ray / per-pixel / per-lot computation is the single-view code, so a
+// view's results in a batch are bit-identical to rendering it alone.
+//
+//   stepViewsK      one thread per view: stepCamera
+//   clearViewsK,
+//   refreshViewsK   clearQueue + prepareLots of all views (grid: slots x views)
+//   buildViewsK     all views' queued lots, one 64-thread block per lot
+//   prologueK       tile bases of every view under the chosen tile order, the
+//                   per-view frame constants (camera basis, sun, origin) and
+//                   the resolve taps, computed once per frame
+//   traceViewsK     persistent: each warp claims `grab` 8x4-pixel tiles at a
+//                   time from a device queue over all views and traces them
+//   shadeViewsK     persistent: shade + resolve of the same tiles, fused
+//
+// The two queues reset themselves: the last warp to find a queue empty zeroes
+// its counters, so consecutive launches (and graph replays) need no memset.
+#include "batch.cuh"
+#include "common_api.cuh"
+#include "hierarchy.cuh"
+#include "traverse.cuh"
+#include "world.cuh"
+
+static_assert(sizeof(stratum_view) == 120, "stratum_view layout is part of the ABI");
+
+namespace st {
+
+__global__ void stepViewsK(stratum_view* V, int n) {
+  int v = int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (v >= n) return;
+  stratum_view& w = V[v];
+  stepOne(w.C, w.Origin, w.I, w.dt, w.width, w.height);
+}
+
+__global__ void clearViewsK(const stratum_view* V, int n) {
+  int v = int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (v < n) V[v].Queue[0] = 0u;
+}
+
+__global__ void refreshViewsK(const stratum_view* __restrict__ V, int n) {
+  int slot = int(blockIdx.x * blockDim.x + threadIdx.x), v = int(blockIdx.y);
+  if (slot >= kLots || v >= n) return;
+  const stratum_view& w = V[v];
+  refreshSlot(slot, w.Origin, int(w.C[14]), w.World, w.Tags, w.Queue);
+}
+
+__global__ void __launch_bounds__(64) buildViewsK(const stratum_view* __restrict__ V, int n) {
+  __shared__ __align__(16) float sm[kNodes][8];
+  const int v = int(blockIdx.y);
+  if (v >= n) return;
+  buildQueue(V[v].Queue, V[v].World, V[v].Nodes, int(blockIdx.x), int(gridDim.x), sm);
+}
+
+__global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
+  if (threadIdx.x == 0) {
+    int base = 0;
+    for (int v = 0; v < n; v++) {
+      V[v].tileBase = base;
+      V[v].tilesX = (V[v].width + kTileW - 1) / kTileW;
+      // a view with no pixels owns no tiles (and is never looked up)
+      if (V[v].width > 0 && V[v].height > 0) base += tileCount(V[v].width, V[v].height, order);
+    }
+    S->counters[kTotalTiles] = uint32_t(base);
+    S->taps = makeTaps();
+  }
+  for (int v = int(threadIdx.x); v < n; v += int(blockDim.x)) S->view[v] = makeFrame(V[v].C, V[v].Origin);
+}
+
+// Last view whose first tile is <= tile (binary search; warp-uniform).
+SD int viewOf(const stratum_view* __restrict__ V, int n, int tile) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (V[mid].tileBase <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Claim `grab` tiles for this warp; returns the first, or >= total when empty.
+SD int claim(uint32_t* next, int grab) {
+  int t0 = 0;
+  if ((threadIdx.x & 31) == 0) t0 = int(atomicAdd(next, uint32_t(grab)));
+  return __shfl_sync(0xffffffffu, t0, 0);
+}
+// The last warp to see the queue empty resets it for the next launch.
+SD void retire(uint32_t* next, uint32_t* done, int threads) {
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence();
+    uint32_t warps = gridDim.x * uint32_t(threads / 32);
+    if (atomicAdd(done, 1u) == warps - 1) { *next = 0u; *done = 0u; }
+  }
+}
+
+// 512 / THREADS resident blocks: at most 128 registers per thread, 16 warps per SM.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS)
+    traceViewsK(const stratum_view* __restrict__ V, int n, int grab, int order, BatchScratch* S) {
+  const int lane = int(threadIdx.x & 31);
+  const int total = int(S->counters[kTotalTiles]);
+#pragma unroll 1
+  for (;;) {
+    const int t0 = claim(&S->counters[kTraceNext], grab);
+    if (t0 >= total) break;
+    const int t1 = min(t0 + grab, total);
+#pragma unroll 1
+    for (int tile = t0; tile < t1; tile++) {
+      const int v = viewOf(V, n, tile);
+      const int W = V[v].width, H = V[v].height;
+      int tx, ty;
+      if (!tileCoord(tile - V[v].tileBase, V[v].tilesX, (H + kTileH - 1) / kTileH, order, tx, ty)) continue;
+      const int x = tx * kTileW + (lane & 7), y = ty * kTileH + (lane >> 3);
+      if (x >= W || y >= H) continue;
+      const Camera cam = S->view[v].cam;
+      const uint32_t o0 = S->view[v].o[0], o2 = S->view[v].o[2];
+      f3 rd = primaryDir(cam, x, y, W, H);
+      TraceResult r = traceRay(V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2, cam.pos, rd,
+                               1.08f / float(H));
+      storeTrace(V[v].Hit, V[v].Surface, size_t(y) * W + x, r);
+    }
+  }
+  retire(&S->counters[kTraceNext], &S->counters[kTraceDone], THREADS);
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) shadeViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
+                                                      BatchScratch* S) {
+  const int lane = int(threadIdx.x & 31);
+  const int total = int(S->counters[kTotalTiles]);
+#pragma unroll 1
+  for (;;) {
+    const int t0 = claim(&S->counters[kShadeNext], grab);
+    if (t0 >= total) break;
+    const int t1 = min(t0 + grab, total);
+#pragma unroll 1
+    for (int tile = t0; tile < t1; tile++) {
+      const int v = viewOf(V, n, tile);
+      const int W = V[v].width, H = V[v].height;
+      int tx, ty;
+      if (!tileCoord(tile - V[v].tileBase, V[v].tilesX, (H + kTileH - 1) / kTileH, order, tx, ty)) continue;
+      const int x = tx * kTileW + (lane & 7), y = ty * kTileH + (lane >> 3);
+      if (x >= W || y >= H) continue;
+      const FrameConst F = S->view[v];
+      const size_t b = size_t(y) * W + x;
+      const float4* hit = reinterpret_cast<const float4*>(V[v].Hit);
+      const float4* surf = reinterpret_cast<const float4*>(V[v].Surface);
+      f3 c = shadePixel(V[v].World, F, hit[b], surf[b], primaryDir(F.cam, x, y, W, H), H);
+      reinterpret_cast<float4*>(V[v].Linear)[b] = make_float4(c.x, c.y, c.z, 1.0f);
+      resolvePixel(c, reinterpret_cast<float4*>(V[v].History), V[v].Pixels, F, S->taps, hit, surf, W, H, x, y);
+    }
+  }
+  retire(&S->counters[kShadeNext], &S->counters[kShadeDone], THREADS);
+}
+
+template <class K>
+int residentBlocks(K kernel, int threads) {
+  int dev = 0, sms = 148, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+  return sms * (per > 0 ? per : 1);
+}
+
+enum Parts { kTrace = 1, kShade = 2 };
+
+template <int T>
+int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratch* S, cudaStream_t s, int parts) {
+  static int traceGrid = 0, shadeGrid = 0;
+  if (!traceGrid) {
+    traceGrid = residentBlocks(traceViewsK<T>, T);
+    shadeGrid = residentBlocks(shadeViewsK<T>, T);
+  }
+  if (parts & kTrace) traceViewsK<T><<<traceGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
+  if (parts & kShade) shadeViewsK<T><<<shadeGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
+  return launchStatus();
+}
+
+bool tuneOk(const stratum_tune& t) {
+  return (t.threads == 64 || t.threads == 128 || t.threads == 256) && t.grab >= 1 && t.grab <= 16 &&
+         (t.order == 0 || t.order == 1);
+}
+
+// parts: kTrace (with the prologue), kShade (uses the prologue's scratch), or both.
+int render(stratum_view* V, int n, void* scratch, unsigned long long bytes, const stratum_tune* tune, cudaStream_t s,
+           int parts) {
+  if (!V || !scratch || n <= 0 || n > 65535 || bytes < batchScratchBytes(n)) return STRATUM_EINVAL;
+  stratum_tune t = tune ? *tune : stratum_tune{128, 1, 1};
+  if (!tuneOk(t)) return STRATUM_EINVAL;
+  BatchScratch* S = static_cast<BatchScratch*>(scratch);
+  if (parts & kTrace) prologueK<<<1, 256, 0, s>>>(V, n, t.order, S);
+  if (t.threads == 64) return launchParts<64>(V, n, t, S, s, parts);
+  if (t.threads == 256) return launchParts<256>(V, n, t, S, s, parts);
+  return launchParts<128>(V, n, t, S, s, parts);
+}
+
+}  // namespace st
+
+using namespace st;
+int stratumHierarchyGrid();
+
+extern "C" {
+
+unsigned long long stratum_batchScratchBytes(int views) { return views > 0 ? batchScratchBytes(views) : 0; }
+
+int stratum_stepViews(stratum_view* views, int n, stratum_stream_t stream) {
+  if (!views || n <= 0) return STRATUM_EINVAL;
+  stepViewsK<<<(n + 63) / 64, 64, 0, asStream(stream)>>>(views, n);
+  return launchStatus();
+}
+int stratum_refreshViews(stratum_view* views, int n, stratum_stream_t stream) {
+  if (!views || n <= 0 || n > 65535) return STRATUM_EINVAL;
+  clearViewsK<<<(n + 63) / 64, 64, 0, asStream(stream)>>>(views, n);
+  refreshViewsK<<<dim3(kLots / 128, n), 128, 0, asStream(stream)>>>(views, n);
+  return launchStatus();
+}
+int stratum_buildViews(stratum_view* views, int n, stratum_stream_t stream) {
+  if (!views || n <= 0 || n > 65535) return STRATUM_EINVAL;
+  int per = stratumHierarchyGrid() / n;
+  buildViewsK<<<dim3(per < 16 ? 16 : per, n), 64, 0, asStream(stream)>>>(views, n);
+  return launchStatus();
+}
+int stratum_traceViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                       const stratum_tune* tune, stratum_stream_t stream) {
+  return render(views, n, scratch, scratchBytes, tune, asStream(stream), kTrace);
+}
+int stratum_shadeViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                       const stratum_tune* tune, stratum_stream_t stream) {
+  return render(views, n, scratch, scratchBytes, tune, asStream(stream), kShade);
+}
+int stratum_renderViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                        const stratum_tune* tune, stratum_stream_t stream) {
+  return render(views, n, scratch, scratchBytes, tune, asStream(stream), kTrace | kShade);
+}
+int stratum_frameViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
+                       const stratum_tune* tune, stratum_stream_t stream) {
+  int s;
+  if ((s = stratum_stepViews(views, n, stream)) != STRATUM_OK) return s;
+  if ((s = stratum_refreshViews(views, n, stream)) != STRATUM_OK) return s;
+  if ((s = stratum_buildViews(views, n, stream)) != STRATUM_OK) return s;
+  return stratum_renderViews(views, n, scratch, scratchBytes, tune, stream);
+}
+
+}  // extern "C"

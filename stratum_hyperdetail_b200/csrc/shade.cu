@@ -33,7 +33,8 @@ __global__ void __launch_bounds__(64) resolveFrameK(const float* __restrict__ Li
   __syncthreads();
   int x = int(blockIdx.x * blockDim.x + threadIdx.x), y = int(blockIdx.y * blockDim.y + threadIdx.y);
   if (x >= width || y >= height) return;
-  resolvePixel(reinterpret_cast<const float4*>(Linear), reinterpret_cast<float4*>(History), Pixels, F, taps,
+  float4 l4 = reinterpret_cast<const float4*>(Linear)[size_t(y) * width + x];
+  resolvePixel(mk(l4.x, l4.y, l4.z), reinterpret_cast<float4*>(History), Pixels, F, taps,
                reinterpret_cast<const float4*>(Hit), reinterpret_cast<const float4*>(Surface), width, height, x, y);
 }
 

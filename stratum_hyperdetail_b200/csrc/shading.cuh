@@ -318,12 +318,12 @@ SD ResolveTaps makeTaps() {
   }
   return r;
 }
-SD void resolvePixel(const float4* __restrict__ Lin, float4* Hist, uint32_t* Px, const FrameConst& F,
-                     const ResolveTaps& taps, const float4* __restrict__ Hit, const float4* __restrict__ Surf,
-                     int width, int height, int x, int y) {
+// `c` is the pixel's linear colour (Linear[b].rgb).
+SD void resolvePixel(f3 c, float4* Hist, uint32_t* Px, const FrameConst& F, const ResolveTaps& taps,
+                     const float4* __restrict__ Hit, const float4* __restrict__ Surf, int width, int height, int x,
+                     int y) {
   const size_t b = size_t(y) * width + x;
-  float4 l4 = Lin[b], h4 = Hit[b];
-  f3 c = mk(l4.x, l4.y, l4.z);
+  float4 h4 = Hit[b];
   if (F.view < 0.5f && int(h4.y) != kSkyId && h4.x < 250.0f) {
     f3 ro = F.cam.pos, point = ro + primaryDir(F.cam, x, y, width, height) * h4.x;
     float4 s4 = Surf[b];

@@ -3,9 +3,14 @@
 #include "common_api.cuh"
 #include "traverse.cuh"
 
+// Minimum resident 64-thread blocks per SM the register allocation must allow.
+#ifndef STRATUM_TRACE_MINB
+#define STRATUM_TRACE_MINB 1
+#endif
+
 namespace st {
 
-__global__ void __launch_bounds__(64) tracePrimaryK(const float* __restrict__ W, const float* __restrict__ N,
+__global__ void __launch_bounds__(64, STRATUM_TRACE_MINB) tracePrimaryK(const float* __restrict__ W, const float* __restrict__ N,
                                                    const uint32_t* __restrict__ O, const float* __restrict__ C,
                                                    float* Hit, float* Surface, int width, int height, int rowStart,
                                                    int rowCount) {

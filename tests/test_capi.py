@@ -37,7 +37,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_python_signatures_cover_header():
     import stratum_hyperdetail_b200 as sb
-    assert set(declared_symbols()) - {"stratum_version"} <= set(sb.SIGNATURES)
+    # the two non-status functions are typed separately in lib()
+    assert set(declared_symbols()) - {"stratum_version", "stratum_batchScratchBytes"} <= set(sb.SIGNATURES)
 
 
 def test_bad_arguments_are_rejected_before_launch():
