@@ -177,6 +177,26 @@ int stratum_shadeViews(stratum_view* views, int n, void* scratch, unsigned long 
  * in *bestMs when not NULL).  Synchronises `stream`. */
 int stratum_autotune(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes, stratum_tune* best,
                      float* bestMs, stratum_stream_t stream);
+/* renderViews for callers that cannot allocate device memory.  No counterpart
+ * in the reference: the reference's engine owns all its buffers, while some
+ * callers of this library cannot hand it a scratch buffer -- an embedding that
+ * gives every byte of HBM to its own pool (a session server that budgets all
+ * memory to per-session tables), a foreign-language binding with no device
+ * allocator, or a frame loop that must not allocate.  This variant keeps the
+ * renderer's scratch (work-queue counters and per-view frame constants) in a
+ * static device array of the library: about 6.9 KB, held by every GPU that
+ * loads the library until the process exits.  It allocates nothing and calls
+ * no allocating routine.
+ * Limits: at most STRATUM_NOALLOC_MAX_VIEWS views per call; more returns
+ * STRATUM_ELIMIT and launches nothing.  The first call on each device looks up
+ * the array's address (cudaGetSymbolAddress); make that first call before any
+ * stream capture on that device.  All calls share the one array: calls whose
+ * work overlaps on the GPU (unordered streams) race and corrupt each other's
+ * frames, so order them on one stream or with events.  Each call clears the
+ * queue counters and rewrites the per-view constants before using them. */
+#define STRATUM_NOALLOC_MAX_VIEWS 64
+#define STRATUM_ELIMIT (-100001) /* request exceeds a fixed capacity of the library */
+int stratum_renderViewsNoAlloc(stratum_view* views, int n, const stratum_tune* tune, stratum_stream_t stream);
 /* The whole batched frame: stepViews, refreshViews, buildViews, renderViews. */
 int stratum_frameViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
                        const stratum_tune* tune, stratum_stream_t stream);

@@ -29,6 +29,8 @@ GROUND_ID = -1
 
 OK = 0
 EINVAL = -100000
+ELIMIT = -100001  # a fixed capacity of the library was exceeded
+NOALLOC_MAX_VIEWS = 64
 QUEUE_STALLED = 1
 BUDGET_EXCEEDED = 2
 NOT_FOUND = 3
@@ -73,6 +75,7 @@ SIGNATURES: dict[str, list] = {
     "stratum_renderViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
     "stratum_frameViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
     "stratum_autotune": [_P, _I, _P, ct.c_ulonglong, _P, _P, _S],
+    "stratum_renderViewsNoAlloc": [_P, _I, _P, _S],
     "stratum_issueProbe": [_P, _I, _I, _S],
 }
 

@@ -58,6 +58,12 @@ class Batch:
     def trace(self, stream=None):
         call("stratum_traceViews", *self._args(), _s(stream))
 
+    def render_no_alloc(self, stream=None):
+        """renderViews through the allocation-free entry point: the library's
+        own static scratch instead of this batch's scratch buffer (at most
+        NOALLOC_MAX_VIEWS views; calls must not overlap on the GPU)."""
+        call("stratum_renderViewsNoAlloc", ptr(self.table), self.n, ct.byref(self.tune), _s(stream))
+
     def shade(self, stream=None):
         call("stratum_shadeViews", *self._args(), _s(stream))
 

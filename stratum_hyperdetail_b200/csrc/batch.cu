@@ -193,7 +193,43 @@ int render(stratum_view* V, int n, void* scratch, unsigned long long bytes, cons
   return launchParts<128>(V, n, t, S, s, parts);
 }
 
+// ---- allocation-free variant -------------------------------------------------
+// The renderer's scratch (queue counters, resolve taps, per-view frame
+// constants) for callers that cannot give the library device memory, held in
+// one static device array.  Every GPU that loads the library holds this array
+// (about 6.9 KB) until the process exits.
+constexpr int kNoAllocMaxViews = STRATUM_NOALLOC_MAX_VIEWS;
+constexpr size_t kNoAllocBytes = sizeof(BatchScratch) + size_t(kNoAllocMaxViews - 1) * sizeof(FrameConst);
+static __device__ __align__(256) unsigned char gNoAllocScratch[kNoAllocBytes];
+
 }  // namespace st
+
+#include <mutex>
+
+namespace {
+// Device address of gNoAllocScratch per device ordinal, looked up on the first
+// call made with that device current.  Host code must not use the array's name
+// as an address: on the host it is only a stand-in for the device symbol.
+constexpr int kMaxDevices = 128;
+std::mutex gNoAllocLock;
+void* gNoAllocAddr[kMaxDevices] = {};
+
+int noAllocScratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return -int(e);
+  if (dev < 0 || dev >= kMaxDevices) return STRATUM_EINVAL;
+  std::lock_guard<std::mutex> hold(gNoAllocLock);
+  if (!gNoAllocAddr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, st::gNoAllocScratch);
+    if (e != cudaSuccess || !p) return e != cudaSuccess ? -int(e) : STRATUM_EINVAL;
+    gNoAllocAddr[dev] = p;
+  }
+  *out = gNoAllocAddr[dev];
+  return STRATUM_OK;
+}
+}  // namespace
 
 using namespace st;
 int stratumHierarchyGrid();
@@ -230,6 +266,19 @@ int stratum_shadeViews(stratum_view* views, int n, void* scratch, unsigned long 
 int stratum_renderViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
                         const stratum_tune* tune, stratum_stream_t stream) {
   return render(views, n, scratch, scratchBytes, tune, asStream(stream), kTrace | kShade);
+}
+// renderViews with the library's static scratch: allocates nothing, calls no
+// allocating routine.  The queue counters are cleared on the stream first, so
+// the call does not depend on how an earlier call ended.
+int stratum_renderViewsNoAlloc(stratum_view* views, int n, const stratum_tune* tune, stratum_stream_t stream) {
+  if (!views || n <= 0) return STRATUM_EINVAL;
+  if (n > kNoAllocMaxViews) return STRATUM_ELIMIT;
+  void* scratch = nullptr;
+  int s = noAllocScratch(&scratch);
+  if (s != STRATUM_OK) return s;
+  cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * kCounters, asStream(stream));
+  if (e != cudaSuccess) return -int(e);
+  return render(views, n, scratch, kNoAllocBytes, tune, asStream(stream), kTrace | kShade);
 }
 int stratum_frameViews(stratum_view* views, int n, void* scratch, unsigned long long scratchBytes,
                        const stratum_tune* tune, stratum_stream_t stream) {
