@@ -19,7 +19,7 @@
 #include "batch.cuh"
 #include "common_api.cuh"
 #include "hierarchy.cuh"
-#include "traverse.cuh"
+#include "traverse_coop.cuh"
 #include "world.cuh"
 
 static_assert(sizeof(stratum_view) == 120, "stratum_view layout is part of the ABI");
@@ -93,10 +93,13 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
 }
 
 // 512 / THREADS resident blocks: at most 128 registers per thread, 16 warps per SM.
+// The warp-cooperative traversal (traverse_coop.cuh) unless built with
+// STRATUM_BATCH_PER_LANE (each lane walks its own ray, as the drop-in kernel).
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS)
     traceViewsK(const stratum_view* __restrict__ V, int n, int grab, int order, BatchScratch* S) {
-  const int lane = int(threadIdx.x & 31);
+  __shared__ StagedFeat feats[THREADS / 32][32];
+  const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
   const int total = int(S->counters[kTotalTiles]);
 #pragma unroll 1
   for (;;) {
@@ -110,12 +113,19 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS)
       int tx, ty;
       if (!tileCoord(tile - V[v].tileBase, V[v].tilesX, (H + kTileH - 1) / kTileH, order, tx, ty)) continue;
       const int x = tx * kTileW + (lane & 7), y = ty * kTileH + (lane >> 3);
-      if (x >= W || y >= H) continue;
+      const bool inFrame = x < W && y < H;
       const Camera cam = S->view[v].cam;
       const uint32_t o0 = S->view[v].o[0], o2 = S->view[v].o[2];
-      f3 rd = primaryDir(cam, x, y, W, H);
+      f3 rd = primaryDir(cam, inFrame ? x : 0, inFrame ? y : 0, W, H);
+#ifdef STRATUM_BATCH_PER_LANE
+      if (!inFrame) continue;
       TraceResult r = traceRay(V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2, cam.pos, rd,
                                1.08f / float(H));
+#else
+      TraceResult r = traceWarp(V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2, cam.pos, rd,
+                                1.08f / float(H), inFrame, feats[warp]);
+      if (!inFrame) continue;
+#endif
       storeTrace(V[v].Hit, V[v].Surface, size_t(y) * W + x, r);
     }
   }

@@ -10,17 +10,25 @@
 // evaluates a trigonometric function for feature placement.
 #include <cmath>
 #include <cstdio>
+#include <initializer_list>
 
 static float host_cos(float a) { volatile float v = a; return std::cos(static_cast<float>(v)); }
 static float host_sin(float a) { volatile float v = a; return std::sin(static_cast<float>(v)); }
 
+// One table per function: a __constant__ copy for the device, a host copy for
+// host builds of the same headers, and an accessor that picks the right one.
+static void one(const char* name, const char* fn, int n, float (*arg)(int), float (*f)(float)) {
+  for (const char* space : {"__constant__", "const"}) {
+    std::printf("static %s float %s%s%s[%d] = {", space, name, fn, space[0] == '_' ? "" : "Host", n);
+    for (int i = 0; i < n; i++) std::printf("%s%a", i ? ", " : "", f(arg(i)));
+    std::printf("};\n");
+  }
+  std::printf("__host__ __device__ __forceinline__ float %s%s(int i) {\n#ifdef __CUDA_ARCH__\n  return %s%s[i];\n"
+              "#else\n  return %s%sHost[i];\n#endif\n}\n", name + 1, fn, name, fn, name, fn);
+}
 static void table(const char* name, int n, float (*arg)(int)) {
-  std::printf("static __constant__ float %sCos[%d] = {", name, n);
-  for (int i = 0; i < n; i++) std::printf("%s%a", i ? ", " : "", host_cos(arg(i)));
-  std::printf("};\n");
-  std::printf("static __constant__ float %sSin[%d] = {", name, n);
-  for (int i = 0; i < n; i++) std::printf("%s%a", i ? ", " : "", host_sin(arg(i)));
-  std::printf("};\n");
+  one(name, "Cos", n, arg, host_cos);
+  one(name, "Sin", n, arg, host_sin);
 }
 
 int main() {

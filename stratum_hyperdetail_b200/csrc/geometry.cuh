@@ -83,12 +83,12 @@ static __device__ __noinline__ float masonryRelief(Feat f, f3 ro, f3 rd, f3 p, f
 }
 
 // Nearest positive hit of one feature, kFar if none (geometry.cu:33-91).
-SD float featureHit(const Feat& f, f3 ro, f3 rd, float cone) {
+// `p`, `d` are the ray in the feature's frame and `inv` = invDir(d); callers
+// that test many features against one ray pass them precomputed.
+SD float featureHitCore(const Feat& f, f3 ro, f3 rd, f3 p, f3 d, f3 inv, float cone) {
   const int shape = f.shape;
   if (shape < 0) return kFar;
   const f3 h = f.h;
-  const f3 p = intoFeature(ro - f.p, f.turn), d = intoFeature(rd, f.turn);
-  const f3 inv = invDir(d);
   Span range = (shape == 3 || shape == 4) ? slabInv(p, inv, mk(-h.x, 0.0f, -h.z), h) : slabInv(p, inv, h * -1.0f, h);
   if (range.hi < fmaxf(0.001f, range.lo)) return kFar;
   float t = range.lo > 0.001f ? range.lo : range.hi;
@@ -164,6 +164,10 @@ SD float featureHit(const Feat& f, f3 ro, f3 rd, float cone) {
   if (t <= 0.001f) return kFar;
   if (shape == 0 && (f.material == 0 || f.material == 1) && h.y > 1.0f) t = masonryRelief(f, ro, rd, p, d, t, cone);
   return t;
+}
+SD float featureHit(const Feat& f, f3 ro, f3 rd, float cone) {
+  const f3 d = intoFeature(rd, f.turn);
+  return featureHitCore(f, ro, rd, intoFeature(ro - f.p, f.turn), d, invDir(d), cone);
 }
 
 // Surface normal of a feature at a point (geometry.cu:92-114).

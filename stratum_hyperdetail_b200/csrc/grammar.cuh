@@ -21,13 +21,13 @@ template <class E> struct Emit {
   float roofBase, roofScale;
   int count;
   // kernels/sink.cu:10-13: features at or above the eave scale vertically.
-  SD void operator()(f3 p, f3 h, int shape, int mat, int turn, float seed) {
+  HD void operator()(f3 p, f3 h, int shape, int mat, int turn, float seed) {
     if (p.y >= roofBase) { p.y = roofBase + (p.y - roofBase) * roofScale; h.y *= roofScale; }
     e.take(Feat{p, h, shape, mat, turn, seed}, count);
     count++;
   }
   // kernels/sink.cu:27-33: a box on facade `face`, pushed `o` out of the wall.
-  SD void wall(int face, float cx, float cz, float w, float d, float u, float y, float o, float hw, float hy, float hd,
+  HD void wall(int face, float cx, float cz, float w, float d, float u, float y, float o, float hw, float hy, float hd,
                int mat, float seed) {
     f3 p = mk(cx + u, y, cz + d + o), h = mk(hw, hy, hd);
     if (face == 1) { p = mk(cx + w + o, y, cz + u); h = mk(hd, hy, hw); }
@@ -39,7 +39,7 @@ template <class E> struct Emit {
 
 // Emits every feature of `group` of `lot` into `sink.take(feature, index)`;
 // returns the feature count.
-template <class E> __device__ __forceinline__ int runGroup(const LotDesc& lot, int group, E& sink) {
+template <class E> HD int runGroup(const LotDesc& lot, int group, E& sink) {
   Emit<E> e{sink, lot.h, lot.roofScale, 0};
   const float x = 0.0f, z = 0.0f, w = lot.w, d = lot.d, h = lot.h, seed = lot.seed, storey = lot.storey;
   const int type = lot.type, mat = lot.mat, floors = lot.floors;
@@ -70,7 +70,7 @@ template <class E> __device__ __forceinline__ int runGroup(const LotDesc& lot, i
         float yy = hash1(int(seed) + j + 991) * 3.3f - 0.5f;
         float rr = sqrtf(hash1(int(seed) + j + 330)) * 2.1f * (1.0f - yy * 0.12f);
         float size = 0.48f + hash1(int(seed) + j + 62) * 0.30f;
-        e(mk(tx + kTreeCos[j] * rr, th + yy, tz + kTreeSin[j] * rr), mk(size, size * 1.25f, size), 1, 7, 0,
+        e(mk(tx + TreeCos(j) * rr, th + yy, tz + TreeSin(j) * rr), mk(size, size * 1.25f, size), 1, 7, 0,
           seed + float(j));
       }
     }
@@ -128,7 +128,7 @@ template <class E> __device__ __forceinline__ int runGroup(const LotDesc& lot, i
         e(mk(xx, h + 16.0f, zz), mk(0.17f, 1.2f, 0.17f), 2, 8, 0, seed);
 #pragma unroll 1
         for (int j = 0; j < 4; j++)
-          e(mk(xx + kQuarterCos[j] * 2.2f, h + 12.0f, zz + kQuarterSin[j] * 2.2f), mk(0.17f, 1.1f, 0.17f), 2, 0, 0,
+          e(mk(xx + QuarterCos(j) * 2.2f, h + 12.0f, zz + QuarterSin(j) * 2.2f), mk(0.17f, 1.1f, 0.17f), 2, 0, 0,
             seed);
       }
     }
@@ -339,7 +339,7 @@ template <class E> __device__ __forceinline__ int runGroup(const LotDesc& lot, i
     }
 #pragma unroll 1
     for (int k = 0; k < 8; k++)
-      e(mk(x + kEighthCos[k] * w * 0.44f, h + 0.42f, z + kEighthSin[k] * d * 0.44f), mk(0.055f, 0.42f, 0.055f), 2, 6, 0,
+      e(mk(x + EighthCos(k) * w * 0.44f, h + 0.42f, z + EighthSin(k) * d * 0.44f), mk(0.055f, 0.42f, 0.055f), 2, 6, 0,
         seed + 840.0f + float(k));
   }
   // street benches and the awnings (assets.cu:252-263)
@@ -370,7 +370,7 @@ template <class E> __device__ __forceinline__ int runGroup(const LotDesc& lot, i
 // Bounds mode (kernels/sink.cu:15-20): AABB union with a 0.025 m pad.
 struct BoundsSink {
   f3 lo{1000000.0f, 1000000.0f, 1000000.0f}, hi{-1000000.0f, -1000000.0f, -1000000.0f};
-  SD void take(const Feat& f, int) {
+  HD void take(const Feat& f, int) {
     f3 ext = f.h;
     if (f.turn % 2 == 1) ext = mk(f.h.z, f.h.y, f.h.x);
     f3 a = f.p - ext, b = f.p + ext;
@@ -384,7 +384,7 @@ struct BoundsSink {
 struct PickSink {
   int target;
   Feat f{mk(0.f, 0.f, 0.f), mk(1.f, 1.f, 1.f), -1, 0, 0, 0.0f};
-  SD void take(const Feat& ft, int id) { if (id == target) f = ft; }
+  HD void take(const Feat& ft, int id) { if (id == target) f = ft; }
 };
 
 }  // namespace st

@@ -12,6 +12,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+// HD: pure functions, also compiled for the host (tests check them against the
+// oracle on the CPU).  SD: device-only helpers.
+#define HD __host__ __device__ __forceinline__
 #define SD __device__ __forceinline__
 
 namespace st {
@@ -35,44 +38,44 @@ constexpr int kGroundId = -1;
 
 // ---- vector type ------------------------------------------------------------
 struct f3 { float x, y, z; };
-SD f3 mk(float x, float y, float z) { return {x, y, z}; }
-SD f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-SD f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-SD f3 operator*(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
-SD f3 operator*(f3 a, f3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
-SD f3 operator/(f3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
-SD float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-SD float len(f3 a) { return sqrtf(dot(a, a)); }
-SD f3 unit(f3 a) { return a / fmaxf(0.000001f, len(a)); }
-SD f3 cross(f3 a, f3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
-SD f3 mix(f3 a, f3 b, float t) { return a + (b - a) * t; }
-SD f3 vmin(f3 a, f3 b) { return {fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)}; }
-SD f3 vmax(f3 a, f3 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)}; }
+HD f3 mk(float x, float y, float z) { return {x, y, z}; }
+HD f3 operator+(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+HD f3 operator-(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+HD f3 operator*(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+HD f3 operator*(f3 a, f3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+HD f3 operator/(f3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+HD float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+HD float len(f3 a) { return sqrtf(dot(a, a)); }
+HD f3 unit(f3 a) { return a / fmaxf(0.000001f, len(a)); }
+HD f3 cross(f3 a, f3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+HD f3 mix(f3 a, f3 b, float t) { return a + (b - a) * t; }
+HD f3 vmin(f3 a, f3 b) { return {fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)}; }
+HD f3 vmax(f3 a, f3 b) { return {fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)}; }
 
 // ---- scalar helpers (common.cu:27-31) ----------------------------------------
-SD float clampv(float x, float a, float b) { return fminf(b, fmaxf(a, x)); }
-SD float sat(float x) { return clampv(x, 0.0f, 1.0f); }
-SD float lerp(float a, float b, float t) { return a + (b - a) * t; }
-SD float fract(float x) { return x - floorf(x); }
-SD float smooth(float a, float b, float x) {
+HD float clampv(float x, float a, float b) { return fminf(b, fmaxf(a, x)); }
+HD float sat(float x) { return clampv(x, 0.0f, 1.0f); }
+HD float lerp(float a, float b, float t) { return a + (b - a) * t; }
+HD float fract(float x) { return x - floorf(x); }
+HD float smooth(float a, float b, float x) {
   float t = sat((x - a) / (b - a));
   return t * t * (3.0f - 2.0f * t);
 }
-SD int imod(int x, int n) { int r = x % n; return r < 0 ? r + n : r; }
+HD int imod(int x, int n) { int r = x % n; return r < 0 ? r + n : r; }
 
 // ---- integer hashing (common.cu:42-44): bit-exact ----------------------------
-SD uint32_t mixbits(uint32_t x) {
+HD uint32_t mixbits(uint32_t x) {
   x ^= x >> 16; x *= 2146121005u; x ^= x >> 15; x *= 2221713035u; x ^= x >> 16;
   return x;
 }
-SD float unit24(uint32_t h) { return float(h & 16777215u) / 16777216.0f; }
-SD float hash1(int x) { return unit24(mixbits(uint32_t(x))); }
-SD float hash2(int x, int y, int seed) {
+HD float unit24(uint32_t h) { return float(h & 16777215u) / 16777216.0f; }
+HD float hash1(int x) { return unit24(mixbits(uint32_t(x))); }
+HD float hash2(int x, int y, int seed) {
   return unit24(mixbits(uint32_t(x) * 1973u + uint32_t(y) * 9277u + uint32_t(seed) * 26699u));
 }
 
 // ---- value noise (common.cu:45-53) ------------------------------------------
-SD float noise2(float x, float y) {
+HD float noise2(float x, float y) {
   int ix = int(floorf(x)), iy = int(floorf(y));
   float fx = fract(x), fy = fract(y);
   fx = fx * fx * (3.0f - 2.0f * fx);
@@ -81,7 +84,7 @@ SD float noise2(float x, float y) {
   float b = lerp(hash2(ix, iy + 1, 13), hash2(ix + 1, iy + 1, 13), fx);
   return lerp(a, b, fy);
 }
-SD float fbm2(float x, float y) {
+HD float fbm2(float x, float y) {
   float v = 0.0f, amp = 0.5f;
 #pragma unroll
   for (int i = 0; i < 5; i++) {
@@ -92,17 +95,17 @@ SD float fbm2(float x, float y) {
   }
   return v;
 }
-SD float freqWeight(float footprint, float freq) { return 1.0f - smooth(0.35f, 1.1f, footprint * freq); }
+HD float freqWeight(float footprint, float freq) { return 1.0f - smooth(0.35f, 1.1f, footprint * freq); }
 
 // ---- camera (common.cu:54-70) -----------------------------------------------
 // sin/cos of the camera angles in double, rounded once to float.
-SD float sinR(float a) { return float(sin(double(a))); }
-SD float cosR(float a) { return float(cos(double(a))); }
+HD float sinR(float a) { return float(sin(double(a))); }
+HD float cosR(float a) { return float(cos(double(a))); }
 struct Camera {
   f3 pos, fwd, right, up;
   float jx, jy;  // Halton jitter of this sample
 };
-SD float halton(int value, int base) {
+HD float halton(int value, int base) {
   float inv = 1.0f / float(base), place = inv, r = 0.0f;
   for (int j = 0; j < 12 && value > 0; j++) {
     r += float(value % base) * place;
@@ -111,7 +114,7 @@ SD float halton(int value, int base) {
   }
   return r;
 }
-SD Camera makeCamera(const float* C) {
+HD Camera makeCamera(const float* C) {
   Camera c;
   c.pos = mk(C[0], C[1], C[2]);
   float s3 = sinR(C[3]), c3 = cosR(C[3]), s4 = sinR(C[4]), c4 = cosR(C[4]);
@@ -123,37 +126,37 @@ SD Camera makeCamera(const float* C) {
   if (sample > 0) { c.jx = halton(sample, 2) - 0.5f; c.jy = halton(sample, 3) - 0.5f; }
   return c;
 }
-SD f3 primaryDir(const Camera& c, int x, int y, int width, int height) {
+HD f3 primaryDir(const Camera& c, int x, int y, int width, int height) {
   float sx = (float(x) + 0.5f + c.jx - float(width) * 0.5f) / float(height) * 1.08f;
   float sy = -(float(y) + 0.5f + c.jy - float(height) * 0.5f) / float(height) * 1.08f;
   return unit(c.fwd + c.right * sx + c.up * sy);
 }
-SD f3 sunDir(const float* C) {
+HD f3 sunDir(const float* C) {
   float s7 = sinR(C[7]), c7 = cosR(C[7]), s8 = sinR(C[8]), c8 = cosR(C[8]);
   return unit(mk(c7 * c8, s8, s7 * c8));
 }
 
 // ---- slab test (common.cu:71-77) --------------------------------------------
-SD float guardedInv(float d) {
+HD float guardedInv(float d) {
   return 1.0f / (fabsf(d) > 0.0000001f ? d : (d < 0.0f ? -0.0000001f : 0.0000001f));
 }
 struct Span { float lo, hi; };
-SD Span slabInv(f3 ro, f3 inv, f3 lo, f3 hi) {
+HD Span slabInv(f3 ro, f3 inv, f3 lo, f3 hi) {
   f3 a = mk((lo.x - ro.x) * inv.x, (lo.y - ro.y) * inv.y, (lo.z - ro.z) * inv.z);
   f3 b = mk((hi.x - ro.x) * inv.x, (hi.y - ro.y) * inv.y, (hi.z - ro.z) * inv.z);
   f3 mn = vmin(a, b), mx = vmax(a, b);
   return {fmaxf(fmaxf(mn.x, mn.y), mn.z), fminf(fminf(mx.x, mx.y), mx.z)};
 }
-SD f3 invDir(f3 rd) { return mk(guardedInv(rd.x), guardedInv(rd.y), guardedInv(rd.z)); }
-SD Span slab(f3 ro, f3 rd, f3 lo, f3 hi) { return slabInv(ro, invDir(rd), lo, hi); }
+HD f3 invDir(f3 rd) { return mk(guardedInv(rd.x), guardedInv(rd.y), guardedInv(rd.z)); }
+HD Span slab(f3 ro, f3 rd, f3 lo, f3 hi) { return slabInv(ro, invDir(rd), lo, hi); }
 
 // ---- masonry relief (common.cu:78-87) ---------------------------------------
-SD void masonryUV(f3 p, f3 n, float& u, float& v) {
+HD void masonryUV(f3 p, f3 n, float& u, float& v) {
   if (fabsf(n.y) > 0.5f) { u = p.x; v = p.z; }
   else if (fabsf(n.x) > 0.5f) { u = p.z; v = p.y; }
   else { u = p.x; v = p.y; }
 }
-SD float masonryHeight(float u, float v, int material) {
+HD float masonryHeight(float u, float v, int material) {
   float bw = material == 1 ? 0.46f : 0.92f, bh = material == 1 ? 0.215f : 0.46f;
   int row = int(floorf(v / bh));
   float x = fract(u / bw + float(imod(row, 2)) * 0.5f), y = fract(v / bh);
@@ -162,7 +165,7 @@ SD float masonryHeight(float u, float v, int material) {
   float chipped = edge - 0.006f * smooth(0.34f, 0.73f, noise2(u * 117.0f, v * 117.0f));
   return -0.018f * (1.0f - smooth(0.008f, 0.023f, chipped)) + 0.0025f * grain;
 }
-SD uint32_t packRGBA8(f3 c) {
+HD uint32_t packRGBA8(f3 c) {
   uint32_t r = uint32_t(sat(c.x) * 255.0f), g = uint32_t(sat(c.y) * 255.0f), b = uint32_t(sat(c.z) * 255.0f);
   return r | (g << 8) | (b << 16) | 4278190080u;
 }
@@ -173,7 +176,7 @@ struct LotDesc {
   float w, d, h; int type, mat, floors; float seed, storey, roofScale; int turn; float ox, oz, palette;
 };
 // 64-bit lot address plus a signed cell offset, carry/borrow per axis.
-SD Addr shiftAddr(uint32_t o0, uint32_t o1, uint32_t o2, uint32_t o3, int dx, int dz) {
+HD Addr shiftAddr(uint32_t o0, uint32_t o1, uint32_t o2, uint32_t o3, int dx, int dz) {
   Addr a;
   a.xl = o0 + uint32_t(dx); a.xh = o1;
   if (dx >= 0 && a.xl < o0) a.xh++;
@@ -183,11 +186,11 @@ SD Addr shiftAddr(uint32_t o0, uint32_t o1, uint32_t o2, uint32_t o3, int dx, in
   if (dz < 0 && a.zl > o2) a.zh--;
   return a;
 }
-SD uint32_t addrKey(Addr a, int seed) {
+HD uint32_t addrKey(Addr a, int seed) {
   return mixbits(a.xl * 1973u + mixbits(a.xh + 719u) + a.zl * 9277u + mixbits(a.zh + 173u) + uint32_t(seed) * 26699u);
 }
-SD float frac16(uint32_t h) { return float(h & 65535u) / 65536.0f; }
-SD LotDesc describe(Addr a, int seed) {
+HD float frac16(uint32_t h) { return float(h & 65535u) / 65536.0f; }
+HD LotDesc describe(Addr a, int seed) {
   uint32_t key = addrKey(a, seed);
   Addr district{(a.xl >> 3) | (a.xh << 29), a.xh >> 3, (a.zl >> 3) | (a.zh << 29), a.zh >> 3};
   uint32_t dk = addrKey(district, seed + 47);
@@ -226,7 +229,7 @@ SD LotDesc loadLot(const float* __restrict__ W, int slot) {
   return l;
 }
 // Plain loads for buffers the same kernel writes (no read-only cache).
-SD LotDesc loadLotRW(const float* W, int slot) {
+HD LotDesc loadLotRW(const float* W, int slot) {
   const float4* s = reinterpret_cast<const float4*>(W + slot * kLotFloats);
   float4 a = s[0], b = s[1], c = s[2], d = s[3];
   LotDesc l;
@@ -236,20 +239,20 @@ SD LotDesc loadLotRW(const float* W, int slot) {
   l.palette = d.x;
   return l;
 }
-SD int tableSlot(uint32_t o0, uint32_t o2, int dx, int dz) {
+HD int tableSlot(uint32_t o0, uint32_t o2, int dx, int dz) {
   int x = int((o0 + uint32_t(dx)) & 127u), z = int((o2 + uint32_t(dz)) & 127u);
   return z * kSide + x;
 }
-SD void slotCell(uint32_t o0, uint32_t o2, int slot, int& cx, int& cz) {
+HD void slotCell(uint32_t o0, uint32_t o2, int slot, int& cx, int& cz) {
   cx = imod(slot % kSide - int(o0 & 127u) + kSide / 2, kSide) - kSide / 2;
   cz = imod(slot / kSide - int(o2 & 127u) + kSide / 2, kSide) - kSide / 2;
 }
-SD f3 toLot(f3 p, int turn) {
+HD f3 toLot(f3 p, int turn) {
   if (turn == 1) return mk(p.z, p.y, -p.x);
   if (turn == 2) return mk(-p.x, p.y, -p.z);
   if (turn == 3) return mk(-p.z, p.y, p.x);
   return p;
 }
-SD f3 fromLot(f3 p, int turn) { return toLot(p, (4 - turn) % 4); }
+HD f3 fromLot(f3 p, int turn) { return toLot(p, (4 - turn) % 4); }
 
 }  // namespace st

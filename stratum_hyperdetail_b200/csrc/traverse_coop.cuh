@@ -1,0 +1,215 @@
+// Warp-cooperative primary traversal for the batched renderer.
+//
+// Same algorithm as traverse.cuh (kernels/trace.cu of the reference), same
+// results bit for bit, organised for a warp of 32 coherent rays (one 8x4 tile):
+//
+//  * each lane advances its own ray -- lot DDA, then the near-first descent of
+//    the lot's hierarchy -- until it reaches a leaf (a group) that must be
+//    evaluated, or finishes;
+//  * the warp then evaluates pending leaves one distinct (lot, group) key at a
+//    time: all 32 lanes build the group's features in shared memory, one
+//    feature per lane (random-access grammar, grammar_ra.cuh), and every lane
+//    waiting on that key tests them in index order with one inlined
+//    intersection routine and its precomputed inverse directions;
+//  * the winner's normal, material and seed are recomputed once per ray.
+//
+// Each lane's leaves are visited in the reference's order and each test sees
+// the same running best, so identity, distance and normal equal the
+// per-thread traversal exactly.  The per-lot hierarchy stack is packed into
+// one 64-bit word (7 bits per node, at most 6 entries).
+#pragma once
+#include "geometry.cuh"
+#include "grammar_ra.cuh"
+#include "traverse.cuh"
+
+namespace st {
+
+// A feature staged in shared memory: three 16-byte words.
+struct alignas(16) StagedFeat {
+  float px, py, pz, hx;
+  float hy, hz;
+  int shape, material;
+  int turn;
+  float seed;
+  int pad0, pad1;
+};
+SD void stage(StagedFeat& s, const Feat& f) {
+  s.px = f.p.x; s.py = f.p.y; s.pz = f.p.z; s.hx = f.h.x; s.hy = f.h.y; s.hz = f.h.z;
+  s.shape = f.shape; s.material = f.material; s.turn = f.turn; s.seed = f.seed;
+}
+SD Feat unstage(const StagedFeat& s) {
+  return Feat{mk(s.px, s.py, s.pz), mk(s.hx, s.hy, s.hz), s.shape, s.material, s.turn, s.seed};
+}
+
+enum LaneState : int { kEnterLot = 0, kInLot = 1, kLeafPending = 2, kDone = 3 };
+
+struct CoopRay {
+  // ray and result
+  f3 ro, rd;
+  float cone, best;
+  int fid, wslot, wcx, wcz;  // winner: group*64+index, slot and DDA cell of its lot
+  // lot DDA
+  float t, tx, tz, dx, dz, farT;
+  int cx, cz, sx, sz, ddaSteps;
+  // current lot
+  int slot, lcx, lcz;
+  f3 lr, ld, inv0, inv1;
+  // hierarchy walk
+  unsigned long long stack;
+  int node, qsteps, pend, state;
+};
+
+SD int popNode(unsigned long long& stack) {
+  int n = int(stack & 127ull);
+  stack >>= 7;
+  return n;
+}
+
+// Ray set-up: ground plane and vertical slab (trace.cu:33-45).
+SD void coopBegin(CoopRay& r, f3 ro, f3 rd, float cone, bool active) {
+  r.ro = ro; r.rd = rd; r.cone = cone;
+  r.best = kFar; r.fid = kSkyId; r.wslot = -1; r.wcx = r.wcz = 0;
+  r.state = active ? kEnterLot : kDone;
+  r.stack = 0ull; r.node = 0; r.qsteps = 0; r.pend = 0; r.slot = 0; r.lcx = r.lcz = 0;
+  r.ddaSteps = 0;
+  if (!active) return;
+  if (rd.y < -0.000001f) {
+    float ground = -ro.y / rd.y;
+    if (ground > 0.001f && ground < r.best) { r.best = ground; r.fid = kGroundId; }
+  }
+  float nearT = 0.001f, farT = r.best;
+  if (fabsf(rd.y) > 0.0000001f) {
+    float a = (-0.5f - ro.y) / rd.y, c = (kTop - ro.y) / rd.y;
+    nearT = fmaxf(nearT, fminf(a, c));
+    farT = fminf(farT, fmaxf(a, c));
+  } else if (ro.y > kTop || ro.y < -0.5f) farT = -1.0f;
+  r.farT = farT;
+  if (!(nearT <= farT)) { r.state = kDone; return; }
+  r.t = nearT + 0.0002f;
+  f3 start = ro + rd * r.t;
+  r.cx = int(floorf((start.x + 18.0f) / kCell));
+  r.cz = int(floorf((start.z + 18.0f) / kCell));
+  r.sx = rd.x > 0.0f ? 1 : -1;
+  r.sz = rd.z > 0.0f ? 1 : -1;
+  float ix = guardedInv(rd.x), iz = guardedInv(rd.z);
+  r.tx = (float(r.cx) * kCell + (r.sx > 0 ? 18.0f : -18.0f) - ro.x) * ix;
+  r.tz = (float(r.cz) * kCell + (r.sz > 0 ? 18.0f : -18.0f) - ro.z) * iz;
+  r.dx = kCell * fabsf(ix);
+  r.dz = kCell * fabsf(iz);
+}
+
+// Advance one lane until it needs a leaf evaluated or is done.
+SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2) {
+#pragma unroll 1
+  while (r.state == kEnterLot || r.state == kInLot) {
+    if (r.state == kEnterLot) {
+      if (r.ddaSteps >= 160 || r.t > r.best || r.t > r.farT || r.t > kFar) { r.state = kDone; break; }
+      r.ddaSteps++;
+      r.slot = tableSlot(o0, o2, r.cx, r.cz);
+      r.lcx = r.cx; r.lcz = r.cz;
+      const float4 c = __ldg(reinterpret_cast<const float4*>(W + r.slot * kLotFloats) + 2);  // roofScale, turn, ox, oz
+      const int turn = int(c.y);
+      f3 cp = mk(float(r.cx) * kCell + c.z, 0.0f, float(r.cz) * kCell + c.w);
+      r.lr = toLot(r.ro - cp, turn);
+      r.ld = toLot(r.rd, turn);
+      r.inv0 = invDir(r.ld);
+      r.inv1 = invDir(mk(r.ld.z, r.ld.y, -r.ld.x));
+      // the DDA steps to the next cell now; the reference does it after the
+      // lot's query, and the next test reads only t and the (later) best
+      if (r.tx < r.tz) { r.t = r.tx; r.tx += r.dx; r.cx += r.sx; } else { r.t = r.tz; r.tz += r.dz; r.cz += r.sz; }
+      if (nodeEntry(N, r.slot * kNodes + 1, r.lr, r.inv0, r.best) < r.best) {
+        r.state = kInLot; r.node = 1; r.stack = 0ull; r.qsteps = 0;
+      }
+      continue;
+    }
+    if (r.node <= 0 || r.qsteps >= kNodes) { r.state = kEnterLot; continue; }
+    r.qsteps++;
+    const int base = r.slot * kNodes;
+    float nearT = nodeEntry(N, base + r.node, r.lr, r.inv0, r.best);
+    if (nearT < r.best && r.node < kGroups) {
+      int left = r.node * 2, right = left + 1;
+      float ln = nodeEntry(N, base + left, r.lr, r.inv0, r.best), rn = nodeEntry(N, base + right, r.lr, r.inv0, r.best);
+      bool lh = ln < r.best, rh = rn < r.best;
+      if (lh && rh) {
+        int next = ln < rn ? left : right, other = ln < rn ? right : left;
+        r.stack = (r.stack << 7) | (unsigned long long)other;
+        r.node = next;
+      } else if (lh) r.node = left;
+      else if (rh) r.node = right;
+      else r.node = popNode(r.stack);
+    } else {
+      if (nearT < r.best && r.node >= kGroups) { r.state = kLeafPending; r.pend = r.node - kGroups; break; }
+      r.node = popNode(r.stack);
+    }
+  }
+}
+
+// One feature against a lane's ray in its lot frame, with the lot's
+// precomputed directions and inverses (turn 0 and turn 1 frames).
+SD float coopHit(const Feat& f, const CoopRay& r) {
+  const bool odd = f.turn % 2 == 1;
+  const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
+  return featureHitCore(f, r.lr, r.ld, intoFeature(r.lr - f.p, f.turn), d, odd ? r.inv1 : r.inv0, r.cone);
+}
+
+// The whole warp traces its 32 rays.  Every lane of the warp must call this
+// (inactive lanes with active = false).  `feats` = 32 staged features of this warp.
+SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
+                         f3 rd, float cone, bool active, StagedFeat* feats) {
+  const int lane = int(threadIdx.x & 31);
+  CoopRay r;
+  coopBegin(r, ro, rd, cone, active);
+#pragma unroll 1
+  for (;;) {
+    coopAdvance(r, W, N, o0, o2);
+    unsigned pending = __ballot_sync(0xffffffffu, r.state == kLeafPending);
+    if (!pending) break;  // every lane is done (lanes only stop advancing at a leaf or when done)
+#pragma unroll 1
+    while (pending) {
+      const int leader = __ffs(pending) - 1;
+      const int key = (r.slot << 6) | r.pend;
+      const int lkey = __shfl_sync(0xffffffffu, key, leader);
+      const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && key == lkey);
+      const int g = lkey & 63;
+      const LotDesc L = loadLot(W, lkey >> 6);
+      const int count = groupCount(L, g);
+      const bool mine = (peers >> lane) & 1u;
+#pragma unroll 1
+      for (int base = 0; base < count; base += 32) {
+        const int j = base + lane;
+        if (j < count) stage(feats[lane], featureAt(L, g, j));
+        __syncwarp();
+        if (mine) {
+          const int m = min(32, count - base);
+#pragma unroll 1
+          for (int k = 0; k < m; k++) {
+            const Feat f = unstage(feats[k]);
+            const float th = coopHit(f, r);
+            if (th > 0.001f && th < r.best) {
+              r.best = th; r.fid = g * kMaxFeatures + base + k; r.wslot = r.slot; r.wcx = r.lcx; r.wcz = r.lcz;
+            }
+          }
+        }
+        __syncwarp();
+      }
+      if (mine) { r.state = kInLot; r.node = popNode(r.stack); }
+      pending &= ~peers;
+    }
+  }
+  TraceResult out;
+  out.t = r.best; out.fid = r.fid; out.material = 10; out.seed = 0.0f; out.slot = -1;
+  out.normal = mk(0.0f, 1.0f, 0.0f);
+  if (r.fid >= 0) {  // the winner's record, lot frame and normal (trace.cu:53-54)
+    const LotDesc L = loadLot(W, r.wslot);
+    const Feat f = featureAt(L, r.fid >> 6, r.fid & 63);
+    f3 cp = mk(float(r.wcx) * kCell + L.ox, 0.0f, float(r.wcz) * kCell + L.oz);
+    f3 lr = toLot(ro - cp, L.turn), ld = toLot(rd, L.turn);
+    out.normal = fromLot(featureNormal(f, lr + ld * r.best), L.turn);
+    out.material = f.material;
+    out.seed = f.seed;
+    out.slot = r.wslot;
+  }
+  return out;
+}
+
+}  // namespace st
