@@ -80,6 +80,8 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=48, help="rows per pose in a CPU sample")
     ap.add_argument("--poses", default=",".join(POSES), help="comma-separated subset of the six poses (profiling)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of each serving run (0: skip)")
+    ap.add_argument("--serve-views", type=int, default=8, help="views per serving batch")
     a = ap.parse_args(argv)
     a.poses = [p for p in a.poses.split(",") if p]
     unknown = set(a.poses) - set(POSES)
@@ -232,6 +234,79 @@ def issue_peak(torch, sb):
     return best
 
 
+def serve_poisson(rate, sessions, duration_s, widths, budget, max_views, streams, tune, seed=1):
+    """Open-loop serving: Poisson arrivals at `rate` requests/s spread uniformly
+    over `sessions` sessions for `duration_s` seconds.  Each session walks its
+    camera through 64-bit lot space at a speed uniform in 1-50 m/s with a yaw
+    drift uniform in +-10 deg/s; every request renders one new sample at the
+    session's current pose.  A warm-up request per session (untimed) admits them
+    all first.  Latency = submit -> frame back in host memory."""
+    from stratum_hyperdetail_b200.server import Pose, Server
+    rng = np.random.default_rng(seed)
+    srv = Server(budget, max_views=max_views, streams=streams, tune=tune)
+    cells = 36.0
+    state = []
+    for i in range(sessions):
+        w = int(widths[rng.integers(len(widths))])
+        h = int(round(w * 9 / 16))
+        sid = srv.open(int(rng.integers(0, 2**31 - 1)), w, h)
+        state.append({"sid": sid, "ox": int(rng.integers(0, 2**64, dtype=np.uint64)),
+                      "oz": int(rng.integers(0, 2**64, dtype=np.uint64)), "x": float(rng.uniform(-18, 18)),
+                      "z": float(rng.uniform(-18, 18)), "y": float(rng.uniform(1.5, 60.0)),
+                      "yaw": float(rng.uniform(0, 2 * math.pi)), "pitch": float(rng.uniform(-0.25, 0.0)),
+                      "speed": float(rng.uniform(1.0, 50.0)), "drift": math.radians(float(rng.uniform(-10, 10))),
+                      "t": 0.0, "w": w, "h": h})
+
+    def pose_at(s, t):
+        dt = t - s["t"]
+        s["t"] = t
+        s["yaw"] += s["drift"] * dt
+        s["x"] += math.sin(s["yaw"]) * s["speed"] * dt
+        s["z"] += math.cos(s["yaw"]) * s["speed"] * dt
+        for axis, o in (("x", "ox"), ("z", "oz")):  # keep the local position inside the cell
+            c = math.floor((s[axis] + 18.0) / cells)
+            s[o] = (s[o] + c) % 2**64
+            s[axis] -= c * cells
+        return Pose.make((s["ox"] & 0xFFFFFFFF, s["ox"] >> 32, s["oz"] & 0xFFFFFFFF, s["oz"] >> 32),
+                         (s["x"], s["y"], s["z"]), s["yaw"], s["pitch"])
+
+    warm = [srv.submit(s["sid"], pose_at(s, 0.0)) for s in state]
+    for r in warm:
+        srv.wait_status(r, 600000)
+    base = srv.stats()
+    times, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration_s:
+            break
+        times.append(t)
+    who = rng.integers(0, sessions, len(times))
+    rids, rays = [], 0
+    t0 = time.perf_counter()
+    for t, k in zip(times, who):
+        lag = t - (time.perf_counter() - t0)
+        if lag > 0:
+            time.sleep(lag)
+        s = state[int(k)]
+        rids.append(srv.submit(s["sid"], pose_at(s, t)))
+        rays += s["w"] * s["h"]
+    lat = []
+    for r in rids:
+        info = srv.wait(r, 600000)
+        if info.status == 0:
+            lat.append(info.latency_ms)
+    span = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array(lat) if lat else np.array([float("nan")])
+    return {"requests": len(rids), "completed": int(len(lat)), "rate_offered": rate, "duration_s": duration_s,
+            "sessions": sessions, "widths": list(widths), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()), "max_ms": float(lat.max()),
+            "rays_per_s": rays / span, "batches": st["batches"] - base["batches"],
+            "admissions": st["admissions"], "evictions": st["evictions"], "budget_gb": budget / 2**30,
+            "resident_gb": st["resident_bytes"] / 2**30, "max_views": max_views, "streams": streams}
+
+
 def timed_steps(torch, stream, steps, flush, body):
     """Run `steps` timed steps: L2 flush (untimed), then `body(events)` between
     two CUDA events on `stream`.  Returns per-step milliseconds and whatever
@@ -377,6 +452,23 @@ def ours_arm(args):
     d2h = sum(t.numel() * 4 for t in host_px)
     e2e_value = rays_per_step * len(e2e_ms) * world / (sum(e2e_ms) * 1e-3)
 
+    # -- serving: continuous batching over resident sessions (open-loop Poisson arrivals)
+    serving = None
+    n_views = len(views)
+    tune_t = (batch.tune.threads, batch.tune.grab, batch.tune.order)
+    batch.graph = None  # release the graph (and, below, the views) before serving and the process group
+    del batch, views
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    if args.serve_seconds > 0 and world == 1:
+        serving = {
+            "mixed_256_sessions": serve_poisson(200.0, 256, args.serve_seconds, (768, 1024, 1600, 1920), 150 << 30,
+                                                args.serve_views, 3, tune_t),
+            "sessions_64_at_1600x900": serve_poisson(200.0, 64, args.serve_seconds, (1600,), 150 << 30,
+                                                     args.serve_views, 3, tune_t, seed=2),
+            "plain_path_per_view_ms": sum(plain_ms) / args.steps / len(names),
+        }
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ol, lib, kind = cpu_lib()
@@ -387,8 +479,6 @@ def ours_arm(args):
 
     if dist:
         dist.barrier()
-    batch.graph = None  # release the graph before the process group
-    if dist:
         dist.destroy_process_group()
     if rank != 0:
         return 0
@@ -398,7 +488,7 @@ def ours_arm(args):
             "data": "synthetic (seeded procedural world, fixed poses)",
             "config": {"workload": "plain single-view frame 1600x900, seed 0x5EED, six poses, one sample per view "
                                    "per step accumulating toward 64",
-                       "width": WIDTH, "height": HEIGHT, "views_per_step": len(views),
+                       "width": WIDTH, "height": HEIGHT, "views_per_step": n_views,
                        "poses": {n: POSES[n] for n in names}, "path": path, "tune": tune,
                        "l2": "flushed between timed steps (256 MiB write outside the timed region)",
                        "parallelism": f"replicas x{world}"},
@@ -411,7 +501,7 @@ def ours_arm(args):
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "call": "stratum_frameViews over the batch, pinned host input and RGBA8 readback"},
-            "gpu_launches": launches, "clocks": clocks.summary(), "wall_s": wall}
+            "gpu_launches": launches, "clocks": clocks.summary(), "wall_s": wall, "serving": serving}
     if not graph_ok:
         line["graph_error"] = graph_err
     print(json.dumps(line), flush=True)

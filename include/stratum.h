@@ -208,6 +208,64 @@ int stratum_frameViews(stratum_view* views, int n, void* scratch, unsigned long 
  * path (its kernels are FP32-issue bound).  `out` receives nothing in practice. */
 int stratum_issueProbe(float* out, int blocks, int iters, stratum_stream_t stream);
 
+/* ---- serving (no reference counterpart: the reference renders one view) --- */
+/* Absolute camera pose: 64-bit lot address per axis and a position (metres)
+ * in that lot's frame, yaw and pitch (radians). */
+typedef struct stratum_pose {
+  unsigned origin[4];
+  float pos[3];
+  float yaw, pitch;
+} stratum_pose;
+
+/* Per view: flags bit 0 = set the pose (C[0..4], Origin), bit 1 = restart
+ * the sample sequence at the next stepCamera (through I[23], the reference's
+ * resize-reset input).  Views, poses and flags are device arrays. */
+int stratum_applyPoses(stratum_view* views, const stratum_pose* poses, const int* flags, int n, stratum_stream_t stream);
+
+typedef struct stratum_server stratum_server;
+typedef struct stratum_server_stats {
+  long long submitted, completed, failed, batches, admissions, evictions;
+  long long resident_sessions;
+  unsigned long long resident_bytes, budget_bytes;
+  double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> frame on the host, completed requests */
+  double rays;                            /* shaded rays rendered */
+  double first_submit_s, last_done_s;     /* wall-clock span of the served requests */
+} stratum_server_stats;
+typedef struct stratum_request_info {
+  int status;          /* STRATUM_OK done, STRATUM_QUEUE_STALLED pending, or an error */
+  int samples_done;
+  double latency_ms;   /* submit -> done */
+  double queue_ms;     /* submit -> first launch */
+} stratum_request_info;
+
+/* A render server on the current device: sessions are admitted while their
+ * device state fits in `budget_bytes`, least recently used idle sessions are
+ * evicted (snapshotted to host memory) to make room, and a scheduler thread
+ * batches up to `max_views` requests per launch over `streams` streams, so a
+ * batch can be forming and launching while others run.  `tune` may be NULL. */
+stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_views, int streams,
+                                      const stratum_tune* tune);
+void stratum_server_destroy(stratum_server* server);
+/* Register a session (not yet resident: admission happens with its first request). */
+int stratum_server_open(stratum_server* server, int seed, int width, int height, int* session);
+int stratum_server_close(stratum_server* server, int session);
+/* Queue `samples` samples of `session` at `pose`.  A pose equal to the
+ * session's previous one keeps accumulating toward 64 samples; a new pose
+ * restarts the sequence.  When the last sample is done its RGBA8 frame is
+ * copied to `out` (width*height*4 bytes, may be NULL). */
+int stratum_server_submit(stratum_server* server, int session, const stratum_pose* pose, int samples,
+                          unsigned char* out, long long* request);
+/* Wait up to timeout_ms for a request: STRATUM_OK when done,
+ * STRATUM_QUEUE_STALLED when the time ran out (the request stays queued). */
+int stratum_server_wait(stratum_server* server, long long request, int timeout_ms, stratum_request_info* info);
+int stratum_server_stats_get(stratum_server* server, stratum_server_stats* stats);
+/* Host-side fault injection for tests: kind 1 = the next `count` session
+ * admissions fail as if the device allocation had failed. */
+int stratum_server_inject(stratum_server* server, int kind, int count);
+/* The last frame (RGBA8) and accumulation buffer of a resident session, copied
+ * to host memory (test and tooling; synchronises the session). */
+int stratum_server_read(stratum_server* server, int session, unsigned char* rgba, float* history);
+
 /* Library version string. */
 const char* stratum_version(void);
 

@@ -33,6 +33,19 @@ __global__ void stepViewsK(stratum_view* V, int n) {
   stepOne(w.C, w.Origin, w.I, w.dt, w.width, w.height);
 }
 
+__global__ void applyPosesK(const stratum_view* V, const stratum_pose* P, const int* flags, int n) {
+  int v = int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (v >= n) return;
+  const stratum_view& w = V[v];
+  const int f = flags[v];
+  if (f & 1) {
+    const stratum_pose& p = P[v];
+    w.C[0] = p.pos[0]; w.C[1] = p.pos[1]; w.C[2] = p.pos[2]; w.C[3] = p.yaw; w.C[4] = p.pitch;
+    for (int i = 0; i < 4; i++) w.Origin[i] = p.origin[i];
+  }
+  const_cast<float*>(w.I)[23] = (f & 2) ? 1.0f : 0.0f;
+}
+
 __global__ void clearViewsK(const stratum_view* V, int n) {
   int v = int(blockIdx.x * blockDim.x + threadIdx.x);
   if (v < n) V[v].Queue[0] = 0u;
@@ -248,6 +261,12 @@ extern "C" {
 
 unsigned long long stratum_batchScratchBytes(int views) { return views > 0 ? batchScratchBytes(views) : 0; }
 
+int stratum_applyPoses(stratum_view* views, const stratum_pose* poses, const int* flags, int n,
+                       stratum_stream_t stream) {
+  if (!views || !poses || !flags || n <= 0) return STRATUM_EINVAL;
+  applyPosesK<<<(n + 63) / 64, 64, 0, asStream(stream)>>>(views, poses, flags, n);
+  return launchStatus();
+}
 int stratum_stepViews(stratum_view* views, int n, stratum_stream_t stream) {
   if (!views || n <= 0) return STRATUM_EINVAL;
   stepViewsK<<<(n + 63) / 64, 64, 0, asStream(stream)>>>(views, n);

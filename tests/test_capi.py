@@ -37,8 +37,14 @@ def test_library_exports_every_declared_symbol():
 
 def test_python_signatures_cover_header():
     import stratum_hyperdetail_b200 as sb
-    # the two non-status functions are typed separately in lib()
-    assert set(declared_symbols()) - {"stratum_version", "stratum_batchScratchBytes"} <= set(sb.SIGNATURES)
+    # the two non-status functions are typed separately in lib(); the server's in server.py
+    names = {n for n in declared_symbols() if not n.startswith("stratum_server_")}
+    assert names - {"stratum_version", "stratum_batchScratchBytes"} <= set(sb.SIGNATURES)
+    from stratum_hyperdetail_b200 import server
+    L = server._lib()
+    for n in declared_symbols():
+        if n.startswith("stratum_server_"):
+            assert getattr(L, n).argtypes is not None, n
 
 
 def test_bad_arguments_are_rejected_before_launch():

@@ -1,0 +1,127 @@
+"""Render server: continuous batching, budget admission, LRU eviction.
+
+Every result must be the same alone and in a mix of concurrent sessions (the
+batched kernels are bit-exact against the single-view path, so the tolerance
+is zero), evicted sessions must continue exactly where they left, and host-side
+failures (admission refused, allocation failure, a wait that times out) must
+leave the server serving.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+MB = 1 << 20
+
+
+def poses_for(k, n, origin=(5, 0, 9, 0)):
+    from stratum_hyperdetail_b200.server import Pose
+    out = []
+    for i in range(n):
+        # stationary for two requests, then a step: exercises accumulation and reset
+        step = i // 2
+        out.append(Pose.make(origin, (10.0 + 3.0 * step + k, 2.0 + k, -4.0 + step), 0.3 * k + 0.1 * step, -0.05))
+    return out
+
+
+def run_alone(seed, w, h, poses, samples=1):
+    from stratum_hyperdetail_b200.server import Server
+    srv = Server(8 << 30, max_views=8, streams=2)
+    sid = srv.open(seed, w, h)
+    out = []
+    for p in poses:
+        rid = srv.submit(sid, p, samples)
+        assert srv.wait_status(rid) == 0
+        out.append(srv.read(sid))
+    srv.close()
+    return out
+
+
+def test_result_is_the_same_alone_and_in_the_mix(cuda):
+    from stratum_hyperdetail_b200.server import Server
+    target = (0x5EED, 192, 108)
+    poses = poses_for(0, 5)
+    alone = run_alone(*target, poses)
+
+    srv = Server(8 << 30, max_views=6, streams=3)
+    sid = srv.open(*target)
+    others = [srv.open(100 + i, 96 + 32 * i, 54 + 18 * i) for i in range(5)]
+    other_poses = [poses_for(i + 1, 5, origin=(i * 1000, 7, 3, i)) for i in range(5)]
+    for k, p in enumerate(poses):
+        rids = [srv.submit(o, other_poses[i][k]) for i, o in enumerate(others[:3])]
+        rid = srv.submit(sid, p)
+        rids += [srv.submit(o, other_poses[i + 3][k]) for i, o in enumerate(others[3:])]
+        assert srv.wait_status(rid) == 0
+        px, hist = srv.read(sid)
+        assert np.array_equal(px, alone[k][0]), f"request {k}: pixels differ in the mix"
+        assert np.array_equal(hist, alone[k][1]), f"request {k}: accumulation differs in the mix"
+        for r in rids:
+            assert srv.wait_status(r) == 0
+    st = srv.stats()
+    assert st["completed"] == 30 and st["failed"] == 0 and st["batches"] >= 5
+    srv.close()
+
+
+def test_served_frame_equals_plain_single_view_path(cuda):
+    from stratum_hyperdetail_b200.server import Pose, Server
+    from stratum_hyperdetail_b200.views import View
+    origin, pos, yaw, pitch = (1, 0, 8, 0), (0.0, 2.0, -16.0), 0.0, 0.0
+    v = View(160, 90)
+    v.set_pose(0x5EED, origin, pos, yaw, pitch)
+    v.frame(0.0)
+    torch.cuda.synchronize()
+    srv = Server(4 << 30, 4, 2)
+    sid = srv.open(0x5EED, 160, 90)
+    assert srv.wait_status(srv.submit(sid, Pose.make(origin, pos, yaw, pitch))) == 0
+    px, hist = srv.read(sid)
+    assert np.array_equal(px, v.Pixels.cpu().numpy().view(np.uint32))
+    assert np.array_equal(hist, v.History.cpu().numpy())
+    srv.close()
+
+
+def test_eviction_and_readmission_continue_exactly(cuda):
+    from stratum_hyperdetail_b200.server import Server
+    sizes = [(160, 90), (128, 72), (144, 81)]
+    poses = [poses_for(i, 6, origin=(i * 77, 0, 3 * i, 0)) for i in range(3)]
+    want = [run_alone(50 + i, *sizes[i], poses[i]) for i in range(3)]
+    one = 66 * MB + max(w * h for w, h in sizes) * 68 + 4 * MB
+    srv = Server(2 * one, max_views=2, streams=2)  # room for two sessions: the third evicts
+    sids = [srv.open(50 + i, *sizes[i]) for i in range(3)]
+    for k in range(6):
+        for i in range(3):
+            rid = srv.submit(sids[i], poses[i][k])
+            assert srv.wait_status(rid) == 0
+            px, hist = srv.read(sids[i])
+            assert np.array_equal(px, want[i][k][0]) and np.array_equal(hist, want[i][k][1]), (i, k)
+    st = srv.stats()
+    assert st["evictions"] >= 6 and st["admissions"] >= 9, st
+    assert st["resident_bytes"] <= st["budget_bytes"]
+    srv.close()
+
+
+def test_budget_refusal_and_injected_allocation_failure(cuda):
+    from stratum_hyperdetail_b200.server import BUDGET_EXCEEDED, Pose, Server
+    srv = Server(150 * MB, max_views=2, streams=1)
+    big = srv.open(1, 1920, 1080)  # needs ~197 MiB: never fits
+    small = srv.open(2, 96, 54)
+    p = Pose.make((0, 0, 0, 0), (14.0, 1.7, 14.0), 0.0, 0.0)
+    assert srv.wait_status(srv.submit(big, p)) == BUDGET_EXCEEDED
+    srv.inject_alloc_failures(1)
+    status = srv.wait_status(srv.submit(small, p))
+    assert status < 0, status  # the failed allocation fails that request only
+    assert srv.wait_status(srv.submit(small, p)) == 0  # and the server keeps serving
+    st = srv.stats()
+    assert st["failed"] == 2 and st["completed"] == 1
+    srv.close()
+
+
+def test_wait_times_out_without_losing_the_request(cuda):
+    from stratum_hyperdetail_b200.server import QUEUE_STALLED, Pose, Server
+    srv = Server(4 << 30, max_views=4, streams=1)
+    sid = srv.open(3, 1600, 900)
+    rid = srv.submit(sid, Pose.make((0, 0, 0, 0), (14.0, 40.0, 14.0), 1.0, -0.2), samples=8)
+    first = srv.wait(rid, timeout_ms=0)
+    assert first.status in (QUEUE_STALLED, 0)
+    info = srv.wait(rid, timeout_ms=30000)
+    assert info.status == 0 and info.samples_done == 8 and info.latency_ms > 0
+    srv.close()
