@@ -105,13 +105,19 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
   }
 }
 
-// 512 / THREADS resident blocks: at most 128 registers per thread, 16 warps per SM.
+// STRATUM_TRACE_OCC / THREADS resident blocks.  768 threads per SM (24 warps,
+// 80 registers per thread with a few spills) measured faster than 512 (128
+// registers, no spills): the traversal is latency-bound.
 // The warp-cooperative traversal (traverse_coop.cuh) unless built with
 // STRATUM_BATCH_PER_LANE (each lane walks its own ray, as the drop-in kernel).
+#ifndef STRATUM_TRACE_OCC
+#define STRATUM_TRACE_OCC 768
+#endif
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS, 512 / THREADS)
+__global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
     traceViewsK(const stratum_view* __restrict__ V, int n, int grab, int order, BatchScratch* S) {
   __shared__ StagedFeat feats[THREADS / 32][32];
+  __shared__ ChunkBox boxes[THREADS / 32][32 / kRun];
   const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
   const int total = int(S->counters[kTotalTiles]);
 #pragma unroll 1
@@ -136,7 +142,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS)
                                1.08f / float(H));
 #else
       TraceResult r = traceWarp(V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2, cam.pos, rd,
-                                1.08f / float(H), inFrame, feats[warp]);
+                                1.08f / float(H), inFrame, feats[warp], boxes[warp]);
       if (!inFrame) continue;
 #endif
       storeTrace(V[v].Hit, V[v].Surface, size_t(y) * W + x, r);

@@ -170,6 +170,26 @@ SD float featureHit(const Feat& f, f3 ro, f3 rd, float cone) {
   return featureHitCore(f, ro, rd, intoFeature(ro - f.p, f.turn), d, invDir(d), cone);
 }
 
+// featureHitCore split for hot loops: the slab test every feature starts with
+// (geometry.cu:37-38) stays inline; what follows a passed slab test is out of
+// line except for plain boxes, so the loop over features stays small in the
+// instruction cache.  featureSlabMiss + featureAfterSlab == featureHitCore.
+SD Span featureSlab(const Feat& f, f3 p, f3 inv) {
+  const f3 h = f.h;
+  return (f.shape == 3 || f.shape == 4) ? slabInv(p, inv, mk(-h.x, 0.0f, -h.z), h) : slabInv(p, inv, h * -1.0f, h);
+}
+SD bool featureSlabMiss(const Feat& f, Span range) { return f.shape < 0 || range.hi < fmaxf(0.001f, range.lo); }
+static __device__ __noinline__ float featureAfterSlabOOL(Feat f, f3 ro, f3 rd, f3 p, f3 d, f3 inv, float cone) {
+  return featureHitCore(f, ro, rd, p, d, inv, cone);
+}
+SD float featureAfterSlab(const Feat& f, f3 ro, f3 rd, f3 p, f3 d, f3 inv, Span range, float cone) {
+  if (f.shape == 0 && !((f.material == 0 || f.material == 1) && f.h.y > 1.0f)) {  // plain box
+    float t = range.lo > 0.001f ? range.lo : range.hi;
+    return t <= 0.001f ? kFar : t;
+  }
+  return featureAfterSlabOOL(f, ro, rd, p, d, inv, cone);
+}
+
 // Surface normal of a feature at a point (geometry.cu:92-114).
 static __device__ __noinline__ f3 featureNormal(Feat f, f3 point) {
   const int shape = f.shape, turn = f.turn;

@@ -24,6 +24,15 @@
 
 namespace st {
 
+// featureAt out of line: one copy, away from the hot test loop in the
+// instruction cache (measured faster than inlining it).
+#ifndef STRATUM_FEATUREAT_INLINE
+static __device__ __noinline__ Feat featureAtOOL(LotDesc L, int g, int i) { return featureAt(L, g, i); }
+#define ST_FEATURE_AT featureAtOOL
+#else
+#define ST_FEATURE_AT featureAt
+#endif
+
 // A feature staged in shared memory: three 16-byte words.
 struct alignas(16) StagedFeat {
   float px, py, pz, hx;
@@ -39,6 +48,27 @@ SD void stage(StagedFeat& s, const Feat& f) {
 }
 SD Feat unstage(const StagedFeat& s) {
   return Feat{mk(s.px, s.py, s.pz), mk(s.hx, s.hy, s.hz), s.shape, s.material, s.turn, s.seed};
+}
+
+// Sub-group culling: every run of kRun staged features gets a box (in the
+// lot frame) that contains every point where any of them can be hit, and a
+// lane tests a run's features only when its ray enters that box nearer than
+// its current best.  Hits lie inside a feature's bounds box (shapes 0-4, 7)
+// or within the 0.025 m masonry pad of it; leaf discs of foliage envelopes can
+// reach one 0.18 m grid cell (0.31 m diagonal) beyond the envelope's box, so
+// foliage gets a 0.35 m pad.  A skipped feature could only have been rejected,
+// so results are unchanged.
+#ifndef STRATUM_COOP_RUN
+#define STRATUM_COOP_RUN 4
+#endif
+constexpr int kRun = STRATUM_COOP_RUN;
+struct ChunkBox { float lo[3], hi[3]; };
+SD void hitBox(const Feat& f, f3& lo, f3& hi) {
+  f3 ext = f.h;
+  if (f.turn % 2 == 1) ext = mk(f.h.z, f.h.y, f.h.x);
+  const float pad = (f.shape == 1 && f.material == 7) ? 0.35f : 0.025f;
+  lo = f.p - ext - mk(pad, pad, pad);
+  hi = f.p + ext + mk(pad, pad, pad);
 }
 
 enum LaneState : int { kEnterLot = 0, kInLot = 1, kLeafPending = 2, kDone = 3 };
@@ -153,9 +183,10 @@ SD float coopHit(const Feat& f, const CoopRay& r) {
 }
 
 // The whole warp traces its 32 rays.  Every lane of the warp must call this
-// (inactive lanes with active = false).  `feats` = 32 staged features of this warp.
+// (inactive lanes with active = false).  `feats` = 32 staged features and
+// `boxes` = 32 / kRun chunk boxes of this warp, in shared memory.
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
-                         f3 rd, float cone, bool active, StagedFeat* feats) {
+                         f3 rd, float cone, bool active, StagedFeat* feats, ChunkBox* boxes) {
   const int lane = int(threadIdx.x & 31);
   CoopRay r;
   coopBegin(r, ro, rd, cone, active);
@@ -176,17 +207,45 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
       const bool mine = (peers >> lane) & 1u;
 #pragma unroll 1
       for (int base = 0; base < count; base += 32) {
+        // stage: lane j builds feature base+j and its hit box; runs of kRun
+        // lanes reduce their boxes into one chunk box
         const int j = base + lane;
-        if (j < count) stage(feats[lane], featureAt(L, g, j));
+        f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
+        if (j < count) {
+          const Feat f = ST_FEATURE_AT(L, g, j);
+          stage(feats[lane], f);
+          hitBox(f, lo, hi);
+        }
+#pragma unroll
+        for (int o = 1; o < kRun; o <<= 1) {
+          lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
+                           __shfl_xor_sync(0xffffffffu, lo.z, o)));
+          hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
+                           __shfl_xor_sync(0xffffffffu, hi.z, o)));
+        }
+        if ((lane & (kRun - 1)) == 0)
+          boxes[lane / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
         __syncwarp();
         if (mine) {
           const int m = min(32, count - base);
 #pragma unroll 1
-          for (int k = 0; k < m; k++) {
-            const Feat f = unstage(feats[k]);
-            const float th = coopHit(f, r);
-            if (th > 0.001f && th < r.best) {
-              r.best = th; r.fid = g * kMaxFeatures + base + k; r.wslot = r.slot; r.wcx = r.lcx; r.wcz = r.lcz;
+          for (int c = 0; c * kRun < m; c++) {
+            const ChunkBox b = boxes[c];
+            const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
+            if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
+            const int kEnd = min(m, (c + 1) * kRun);
+#pragma unroll 1
+            for (int k = c * kRun; k < kEnd; k++) {
+              const Feat f = unstage(feats[k]);
+              const bool odd = f.turn % 2 == 1;
+              const f3 inv = odd ? r.inv1 : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
+              const Span rg = featureSlab(f, p, inv);
+              if (featureSlabMiss(f, rg)) continue;
+              const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
+              const float th = featureAfterSlab(f, r.lr, r.ld, p, d, inv, rg, r.cone);
+              if (th > 0.001f && th < r.best) {  // index order: the first feature wins ties
+                r.best = th; r.fid = g * kMaxFeatures + base + k; r.wslot = r.slot; r.wcx = r.lcx; r.wcz = r.lcz;
+              }
             }
           }
         }
