@@ -116,8 +116,8 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
     traceViewsK(const stratum_view* __restrict__ V, int n, int grab, int order, BatchScratch* S) {
-  __shared__ StagedFeat feats[THREADS / 32][32];
-  __shared__ ChunkBox boxes[THREADS / 32][32 / kRun];
+  __shared__ StagedFeat feats[THREADS / 32][kKeys * kKeyStride];
+  __shared__ ChunkBox boxes[THREADS / 32][kKeys * (32 / kRun)];
   const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
   const int total = int(S->counters[kTotalTiles]);
 #pragma unroll 1

@@ -33,22 +33,33 @@ static __device__ __noinline__ Feat featureAtOOL(LotDesc L, int g, int i) { retu
 #define ST_FEATURE_AT featureAt
 #endif
 
-// A feature staged in shared memory: three 16-byte words.
+// A feature staged in shared memory: two 16-byte words; shape (+1), material
+// and turn packed into one (shape >= -1, material and turn in [0, 255]).
 struct alignas(16) StagedFeat {
   float px, py, pz, hx;
   float hy, hz;
-  int shape, material;
-  int turn;
+  int packed;
   float seed;
-  int pad0, pad1;
 };
 SD void stage(StagedFeat& s, const Feat& f) {
   s.px = f.p.x; s.py = f.p.y; s.pz = f.p.z; s.hx = f.h.x; s.hy = f.h.y; s.hz = f.h.z;
-  s.shape = f.shape; s.material = f.material; s.turn = f.turn; s.seed = f.seed;
+  s.packed = (f.shape + 1) | (f.material << 8) | (f.turn << 16);
+  s.seed = f.seed;
 }
 SD Feat unstage(const StagedFeat& s) {
-  return Feat{mk(s.px, s.py, s.pz), mk(s.hx, s.hy, s.hz), s.shape, s.material, s.turn, s.seed};
+  return Feat{mk(s.px, s.py, s.pz), mk(s.hx, s.hy, s.hz), (s.packed & 255) - 1, (s.packed >> 8) & 255,
+              (s.packed >> 16) & 255, s.seed};
 }
+// Keys (distinct lot, group pairs) a warp evaluates at once, and the staged
+// stride per key: 33 records, so the same record index of different keys falls
+// in different shared-memory banks.  One key at a time measured fastest on the
+// benchmark poses (2 and 4 keys: 9 % and 19 % slower): staging several keys
+// costs more than the extra lanes it keeps busy.
+#ifndef STRATUM_COOP_KEYS
+#define STRATUM_COOP_KEYS 1
+#endif
+constexpr int kKeys = STRATUM_COOP_KEYS;
+constexpr int kKeyStride = 33;
 
 // Sub-group culling: every run of kRun staged features gets a box (in the
 // lot frame) that contains every point where any of them can be hit, and a
@@ -183,8 +194,10 @@ SD float coopHit(const Feat& f, const CoopRay& r) {
 }
 
 // The whole warp traces its 32 rays.  Every lane of the warp must call this
-// (inactive lanes with active = false).  `feats` = 32 staged features and
-// `boxes` = 32 / kRun chunk boxes of this warp, in shared memory.
+// (inactive lanes with active = false).  `feats` = kKeys * kKeyStride staged
+// records and
+// `boxes` = kKeys * 32 / kRun chunk boxes of this warp, in shared memory
+// (staged records at key * kKeyStride).
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
                          f3 rd, float cone, bool active, StagedFeat* feats, ChunkBox* boxes) {
   const int lane = int(threadIdx.x & 31);
@@ -197,46 +210,72 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
     if (!pending) break;  // every lane is done (lanes only stop advancing at a leaf or when done)
 #pragma unroll 1
     while (pending) {
-      const int leader = __ffs(pending) - 1;
+      // Take up to kKeys distinct keys among the pending lanes.
       const int key = (r.slot << 6) | r.pend;
-      const int lkey = __shfl_sync(0xffffffffu, key, leader);
-      const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && key == lkey);
-      const int g = lkey & 63;
-      const LotDesc L = loadLot(W, lkey >> 6);
-      const int count = groupCount(L, g);
-      const bool mine = (peers >> lane) & 1u;
-#pragma unroll 1
-      for (int base = 0; base < count; base += 32) {
-        // stage: lane j builds feature base+j and its hit box; runs of kRun
-        // lanes reduce their boxes into one chunk box
-        const int j = base + lane;
-        f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
-        if (j < count) {
-          const Feat f = ST_FEATURE_AT(L, g, j);
-          stage(feats[lane], f);
-          hitBox(f, lo, hi);
-        }
+      int keys[kKeys];
+      unsigned batch = 0u;
+      int myq = -1;
 #pragma unroll
-        for (int o = 1; o < kRun; o <<= 1) {
-          lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
-                           __shfl_xor_sync(0xffffffffu, lo.z, o)));
-          hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
-                           __shfl_xor_sync(0xffffffffu, hi.z, o)));
+      for (int q = 0; q < kKeys; q++) {
+        keys[q] = -1;
+        const unsigned rem = pending & ~batch;
+        if (rem) {
+          const int kq = __shfl_sync(0xffffffffu, key, __ffs(rem) - 1);
+          const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && key == kq);
+          keys[q] = kq;
+          batch |= peers;
+          if ((peers >> lane) & 1u) myq = q;
         }
-        if ((lane & (kRun - 1)) == 0)
-          boxes[lane / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
+      }
+      int myCount = 0, maxCount = 0;
+#pragma unroll
+      for (int q = 0; q < kKeys; q++)
+        if (keys[q] >= 0) {
+          const int c = groupCount(loadLot(W, keys[q] >> 6), keys[q] & 63);
+          if (myq == q) myCount = c;
+          maxCount = max(maxCount, c);
+        }
+      const int g = r.pend;
+#pragma unroll 1
+      for (int base = 0; base < maxCount; base += 32) {
+        // stage, key by key: lane j builds feature base+j of the key and its
+        // hit box; runs of kRun lanes reduce their boxes into one chunk box
+#pragma unroll
+        for (int q = 0; q < kKeys; q++) {
+          if (keys[q] < 0) break;
+          const LotDesc L = loadLot(W, keys[q] >> 6);
+          const int gq = keys[q] & 63, count = groupCount(L, gq), j = base + lane;
+          f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
+          if (j < count) {
+            const Feat f = ST_FEATURE_AT(L, gq, j);
+            stage(feats[q * kKeyStride + lane], f);
+            hitBox(f, lo, hi);
+          }
+#pragma unroll
+          for (int o = 1; o < kRun; o <<= 1) {
+            lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
+                             __shfl_xor_sync(0xffffffffu, lo.z, o)));
+            hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
+                             __shfl_xor_sync(0xffffffffu, hi.z, o)));
+          }
+          if ((lane & (kRun - 1)) == 0)
+            boxes[q * (32 / kRun) + lane / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
+        }
         __syncwarp();
-        if (mine) {
-          const int m = min(32, count - base);
+        // every waiting lane tests its own key's staged features
+        if (myq >= 0 && base < myCount) {
+          const StagedFeat* fq = feats + myq * kKeyStride;
+          const ChunkBox* bq = boxes + myq * (32 / kRun);
+          const int m = min(32, myCount - base);
 #pragma unroll 1
           for (int c = 0; c * kRun < m; c++) {
-            const ChunkBox b = boxes[c];
+            const ChunkBox b = bq[c];
             const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
             if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
             const int kEnd = min(m, (c + 1) * kRun);
 #pragma unroll 1
             for (int k = c * kRun; k < kEnd; k++) {
-              const Feat f = unstage(feats[k]);
+              const Feat f = unstage(fq[k]);
               const bool odd = f.turn % 2 == 1;
               const f3 inv = odd ? r.inv1 : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
               const Span rg = featureSlab(f, p, inv);
@@ -251,8 +290,8 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
         }
         __syncwarp();
       }
-      if (mine) { r.state = kInLot; r.node = popNode(r.stack); }
-      pending &= ~peers;
+      if (myq >= 0) { r.state = kInLot; r.node = popNode(r.stack); }
+      pending &= ~batch;
     }
   }
   TraceResult out;
