@@ -120,6 +120,14 @@ int stratum_enumerateGroups(const float* Lots, const int* Groups, int pairs, int
  * Results n x [t, normal.xyz] (kernels/geometry.cu:33,92). */
 int stratum_featureQuery(const float* Queries, int n, float* Results, stratum_stream_t stream);
 
+/* Nearest hit of n arbitrary rays in a view's table (kernels/trace.cu:8-61):
+ * Rays n x 7 f32 [ro.xyz, rd.xyz, cone] in the floating-origin frame; Out
+ * n x 8 f32 [t, fid, material, seed, normal.xyz, slot].  exhaustive = 1
+ * evaluates every group of every visited lot (no hierarchy culling; Nodes may
+ * be NULL): the check of the hierarchy (tests/native_harness.cpp:68-79). */
+int stratum_traceRays(const float* World, const float* Nodes, const unsigned* Origin, const float* Rays, int n,
+                      int exhaustive, float* Out, stratum_stream_t stream);
+
 /* ---- batched views (no reference counterpart: B200 multi-view form) ------- */
 /* One view of a batch: device pointers to that view's own buffers, in the
  * layouts above, plus its frame size and time step.  A batch is a DEVICE array

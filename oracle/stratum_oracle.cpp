@@ -896,6 +896,63 @@ void tracePixel(const float* W, const float* N, const uint32_t* O, const float* 
   if (second) second[y * width + x] = (cand.a == best) ? cand.b : cand.a;
 }
 
+// An arbitrary ray through the table (trace.cu:33-61); with `exhaustive` every
+// group of each visited lot is evaluated in index order instead of walking the
+// hierarchy.  out8 = [t, fid, material, seed, n.xyz, slot].
+void traceRayOrc(const float* W, const float* N, const uint32_t* O, V3f ro, V3f rd, float cone, bool exhaustive,
+                 float* out8) {
+  float best = kFar, seed = 0.0f;
+  int fid = -10000, material = 10, found = -1;
+  V3f normal = mk(0.0f, 1.0f, 0.0f);
+  if (rd.y < -0.000001f) {
+    float ground = -ro.y / rd.y;
+    if (ground > 0.001f && ground < best) { best = ground; fid = -1; }
+  }
+  float nearT = 0.001f, farT = best;
+  if (std::fabs(rd.y) > 0.0000001f) {
+    float a = (-0.5f - ro.y) / rd.y, c = (kTop - ro.y) / rd.y;
+    nearT = std::fmax(nearT, std::fmin(a, c));
+    farT = std::fmin(farT, std::fmax(a, c));
+  } else if (ro.y > kTop || ro.y < -0.5f) farT = -1.0f;
+  if (nearT <= farT) {
+    float t = nearT + 0.0002f;
+    V3f start = ro + rd * t;
+    int cx = int(std::floor((start.x + 18.0f) / kCell)), cz = int(std::floor((start.z + 18.0f) / kCell));
+    int sx = rd.x > 0.0f ? 1 : -1, sz = rd.z > 0.0f ? 1 : -1;
+    float tx = (float(cx) * kCell + (sx > 0 ? 18.0f : -18.0f) - ro.x) * guardedInv(rd.x);
+    float tz = (float(cz) * kCell + (sz > 0 ? 18.0f : -18.0f) - ro.z) * guardedInv(rd.z);
+    float dx = kCell * std::fabs(guardedInv(rd.x)), dz = kCell * std::fabs(guardedInv(rd.z));
+    for (int step = 0; step < 160; step++) {
+      if (t > best || t > farT || t > kFar) break;
+      int slot = tableSlot(O, cx, cz);
+      LotDesc lot = loadLot(W, slot);
+      V3f cp = mk(float(cx) * kCell + lot.ox, 0.0f, float(cz) * kCell + lot.oz);
+      V3f lr = toLot(ro - cp, lot.turn), ld = toLot(rd, lot.turn);
+      if (exhaustive) {
+        for (int g = 0; g < kGroups; g++) {
+          float th; int id; Feat f;
+          groupNearest(lot, g, lr, ld, cone, best, th, id, f, nullptr, nullptr);
+          if (id >= 0 && th < best) {
+            best = th; fid = g * kMaxFeatures + id; material = f.material; seed = f.seed;
+            normal = fromLot(featNormal<float>(f, lr + ld * best), lot.turn);
+            found = slot;
+          }
+        }
+      } else if (nodeEntry(N, slot * kNodes + 1, lr, ld, best, nullptr) < best) {
+        Nearest hit = queryLotNearest(lot, N, slot, lr, ld, best, cone, nullptr, nullptr);
+        if (hit.fid >= 0 && hit.t < best) {
+          best = hit.t; fid = hit.fid; material = hit.f.material; seed = hit.f.seed;
+          normal = fromLot(featNormal<float>(hit.f, lr + ld * best), lot.turn);
+          found = slot;
+        }
+      }
+      if (tx < tz) { t = tx; tx += dx; cx += sx; } else { t = tz; tz += dz; cz += sz; }
+    }
+  }
+  out8[0] = best; out8[1] = float(fid); out8[2] = float(material); out8[3] = seed;
+  out8[4] = normal.x; out8[5] = normal.y; out8[6] = normal.z; out8[7] = float(found);
+}
+
 // ---- materials (materials.cu) ----------------------------------------------
 inline V3f substrateMean(int m) { return m == 1 ? mk(0.37f, 0.185f, 0.105f) : mk(0.55f, 0.485f, 0.365f); }
 V3f substrate(float u, float v, float seed, int m) {
@@ -1397,6 +1454,14 @@ void orc_resolveFrame(const float* Lin, float* Hist, uint32_t* Px, const float* 
 #pragma omp parallel for schedule(dynamic, 2) num_threads(useThreads(nthreads))
   for (int y = 0; y < height; y++)
     for (int x = 0; x < width; x++) resolvePixel(Lin, Hist, Px, C, Hit, Surf, width, height, x, y);
+}
+void orc_traceRays(const float* W, const float* N, const uint32_t* O, const float* rays, int n, int exhaustive,
+                   float* out, int nthreads) {
+#pragma omp parallel for schedule(dynamic, 16) num_threads(useThreads(nthreads))
+  for (int i = 0; i < n; i++) {
+    const float* q = rays + size_t(i) * 7;
+    traceRayOrc(W, N, O, mk(q[0], q[1], q[2]), mk(q[3], q[4], q[5]), q[6], exhaustive != 0, out + size_t(i) * 8);
+  }
 }
 void orc_resolveRows(const float* Lin, float* Hist, uint32_t* Px, const float* C, const float* Hit, const float* Surf,
                      int width, int height, int rowStart, int rowCount, int nthreads) {

@@ -71,6 +71,9 @@ void orc_shadePixels(const float* World, const uint32_t* Origin, const float* C,
                      int nthreads, int64_t* counters);
 void orc_resolveFrame(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
                       const float* Surface, int width, int height, int nthreads);
+/* rays: n x 7 [ro.xyz, rd.xyz, cone]; out: n x 8 [t, fid, material, seed, n.xyz, slot] */
+void orc_traceRays(const float* World, const float* Nodes, const uint32_t* Origin, const float* rays, int n,
+                   int exhaustive, float* out, int nthreads);
 void orc_resolveRows(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
                      const float* Surface, int width, int height, int rowStart, int rowCount, int nthreads);
 void orc_probeGrammar(const float* Inputs, float* Output);

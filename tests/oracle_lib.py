@@ -137,6 +137,7 @@ class Oracle(_Lib):
                                       ct.c_int, ct.c_void_p]
         L.orc_resolveFrame.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p, ct.c_int, ct.c_int, ct.c_int]
         L.orc_resolveRows.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p] + [ct.c_int] * 5
+        L.orc_traceRays.argtypes = [f32p, f32p, u32p, f32p, ct.c_int, ct.c_int, f32p, ct.c_int]
         L.orc_featureHit_f64.restype = ct.c_double
         L.orc_featureHit_f64.argtypes = [f32p, f64p, f64p, ct.c_double]
         L.orc_featureNormal_f64.argtypes = [f32p, f64p, f64p]
@@ -163,6 +164,14 @@ class Oracle(_Lib):
 
     def resolve_rows(self, linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads=0):
         self.lib.orc_resolveRows(linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads)
+
+    def trace_rays(self, world, nodes, origin, rays, exhaustive=False, nthreads=0):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        out = np.zeros((n, 8), np.float32)
+        self.lib.orc_traceRays(world, nodes, np.ascontiguousarray(origin, np.uint32), rays, n, int(exhaustive), out,
+                               nthreads)
+        return out
 
     def feature_hit_f64(self, f10, ro, rd, cone=0.0):
         return self.lib.orc_featureHit_f64(np.ascontiguousarray(f10, np.float32), np.ascontiguousarray(ro, np.float64),
