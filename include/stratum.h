@@ -145,10 +145,23 @@ typedef struct stratum_view {
   float* Linear;
   float* History;
   unsigned* Pixels;
+  unsigned* Groups; /* the table's group cache (stratum_groupCacheInit), or NULL */
   int width, height;
   float dt;
   int tileBase, tilesX, reserved;
 } stratum_view;
+
+/* Group cache of one table: the feature records of the (lot, group) pairs the
+ * batched trace has evaluated, filled on first use and loaded afterwards
+ * instead of being rebuilt by the grammar.  `entries` groups of at most 56
+ * records (1,856 bytes each) plus a 4 MiB directory.  Entries are checked
+ * against the table's current descriptor rows, so the cache never needs
+ * invalidating when the table is refreshed (by any entry point); a full cache
+ * is emptied at the start of the next batched frame.  Results are identical
+ * with and without a cache.  Initialise once before use (zeroes the directory,
+ * sets the capacity); a zero-filled buffer is a cache of capacity 0. */
+unsigned long long stratum_groupCacheBytes(int entries);
+int stratum_groupCacheInit(unsigned* Groups, int entries, stratum_stream_t stream);
 
 /* Tunables of the batched trace: block size (64/128/256), tiles a warp claims
  * per queue access (queue depth, 1..16), tile order within a view (0 row-major,
@@ -254,6 +267,9 @@ typedef struct stratum_request_info {
 stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_views, int streams,
                                       const stratum_tune* tune);
 void stratum_server_destroy(stratum_server* server);
+/* Group cache entries of every session's table (default 65,536: 120 MiB per
+ * session, counted in the budget; 0: none).  Only before the first open. */
+int stratum_server_set_group_cache(stratum_server* server, int entries);
 /* Register a session (not yet resident: admission happens with its first request). */
 int stratum_server_open(stratum_server* server, int seed, int width, int height, int* session);
 int stratum_server_close(stratum_server* server, int session);

@@ -31,6 +31,7 @@ OK = 0
 EINVAL = -100000
 ELIMIT = -100001  # a fixed capacity of the library was exceeded
 NOALLOC_MAX_VIEWS = 64
+GROUP_CACHE_ENTRIES = 65536  # default group cache of a batched view: 116 MiB + 4 MiB directory
 QUEUE_STALLED = 1
 BUDGET_EXCEEDED = 2
 NOT_FOUND = 3
@@ -78,6 +79,7 @@ SIGNATURES: dict[str, list] = {
     "stratum_frameViews": [_P, _I, _P, ct.c_ulonglong, _P, _S],
     "stratum_autotune": [_P, _I, _P, ct.c_ulonglong, _P, _P, _S],
     "stratum_renderViewsNoAlloc": [_P, _I, _P, _S],
+    "stratum_groupCacheInit": [_P, _I, _S],
     "stratum_issueProbe": [_P, _I, _I, _S],
 }
 
@@ -90,7 +92,7 @@ class Tune(ct.Structure):
 class ViewRecord(ct.Structure):
     """stratum_view: one view of a batch (device pointers + size)."""
     _fields_ = [(n, ct.c_void_p) for n in ("C", "Origin", "I", "World", "Tags", "Nodes", "Queue", "Hit", "Surface",
-                                            "Linear", "History", "Pixels")] + [
+                                            "Linear", "History", "Pixels", "Groups")] + [
         ("width", ct.c_int), ("height", ct.c_int), ("dt", ct.c_float), ("tileBase", ct.c_int), ("tilesX", ct.c_int),
         ("reserved", ct.c_int)]
 
@@ -112,6 +114,8 @@ def lib() -> ct.CDLL:
         L.stratum_version.argtypes = []
         L.stratum_batchScratchBytes.restype = ct.c_ulonglong
         L.stratum_batchScratchBytes.argtypes = [ct.c_int]
+        L.stratum_groupCacheBytes.restype = ct.c_ulonglong
+        L.stratum_groupCacheBytes.argtypes = [ct.c_int]
         _lib = L
     return _lib
 

@@ -11,7 +11,7 @@ import ctypes as ct
 
 import torch
 
-from . import Tune, ViewRecord, call, lib, ptr
+from . import GROUP_CACHE_ENTRIES, Tune, ViewRecord, call, lib, ptr
 from .views import View
 
 
@@ -20,15 +20,20 @@ def _s(stream):
 
 
 class Batch:
-    def __init__(self, views: list[View], tune: tuple[int, int, int] = (128, 1, 1), device="cuda"):
+    def __init__(self, views: list[View], tune: tuple[int, int, int] = (128, 1, 1), device="cuda",
+                 group_cache: int = GROUP_CACHE_ENTRIES):
+        """`group_cache`: entries of the group cache given to every view that has
+        none yet (0: views without a cache stay without one)."""
         if not views:
             raise ValueError("a batch needs at least one view")
         self.views = list(views)
         self.n = len(self.views)
         rec = (ViewRecord * self.n)()
         for r, v in zip(rec, self.views):
+            if group_cache > 0 and v.Groups is None:
+                v.enable_group_cache(group_cache)
             for name in ("C", "Origin", "I", "World", "Tags", "Nodes", "Queue", "Hit", "Surface", "Linear",
-                         "History", "Pixels"):
+                         "History", "Pixels", "Groups"):
                 setattr(r, name, ptr(getattr(v, name)))
             r.width, r.height, r.dt = v.width, v.height, 0.0
         raw = bytes(rec)
@@ -86,8 +91,8 @@ class Batch:
 
     @property
     def launches_per_frame(self) -> int:
-        # stepViews, clearViews, refreshViews, buildViews, prologue, trace, shade
-        return 7
+        # stepViews, clearViews, refreshViews, buildViews, cacheReset, prologue, trace, shade
+        return 8
 
     def capture(self):
         """Capture one batched frame as a CUDA graph (after one eager frame so

@@ -7,6 +7,7 @@
 //   clearViewsK,
 //   refreshViewsK   clearQueue + prepareLots of all views (grid: slots x views)
 //   buildViewsK     all views' queued lots, one 64-thread block per lot
+//   cacheResetK     empties the group caches that filled up (group_cache.cuh)
 //   prologueK       tile bases of every view under the chosen tile order, the
 //                   per-view frame constants (camera basis, sun, origin) and
 //                   the resolve taps, computed once per frame
@@ -22,7 +23,7 @@
 #include "traverse_coop.cuh"
 #include "world.cuh"
 
-static_assert(sizeof(stratum_view) == 120, "stratum_view layout is part of the ABI");
+static_assert(sizeof(stratum_view) == 128, "stratum_view layout is part of the ABI");
 
 namespace st {
 
@@ -65,6 +66,22 @@ __global__ void __launch_bounds__(64) buildViewsK(const stratum_view* __restrict
   buildQueue(V[v].Queue, V[v].World, V[v].Nodes, int(blockIdx.x), int(gridDim.x), sm);
 }
 
+// A full group cache is emptied at the start of a frame: its directory is
+// zeroed here, its fill counter reset by the prologue that follows.
+__global__ void cacheResetK(const stratum_view* __restrict__ V, int n) {
+  const int v = int(blockIdx.y);
+  if (v >= n || !V[v].Groups) return;
+  const GroupCache c = groupCache(V[v].Groups);
+  if (c.capacity == 0u || c.hdr->next < c.capacity) return;
+  uint4* d = reinterpret_cast<uint4*>(c.dir);
+  for (int i = int(blockIdx.x * blockDim.x + threadIdx.x); i < kCacheDirWords / 4; i += int(gridDim.x * blockDim.x))
+    d[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+__global__ void cacheInitK(uint32_t* base, uint32_t entries) {
+  GroupCacheHeader* h = reinterpret_cast<GroupCacheHeader*>(base);
+  h->next = 0u; h->capacity = entries; h->resets = 0u; h->fills = 0u;
+}
+
 __global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
   if (threadIdx.x == 0) {
     int base = 0;
@@ -77,7 +94,13 @@ __global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
     S->counters[kTotalTiles] = uint32_t(base);
     S->taps = makeTaps();
   }
-  for (int v = int(threadIdx.x); v < n; v += int(blockDim.x)) S->view[v] = makeFrame(V[v].C, V[v].Origin);
+  for (int v = int(threadIdx.x); v < n; v += int(blockDim.x)) {
+    S->view[v] = makeFrame(V[v].C, V[v].Origin);
+    if (V[v].Groups) {  // after cacheResetK: a full cache starts again
+      GroupCacheHeader* h = reinterpret_cast<GroupCacheHeader*>(V[v].Groups);
+      if (h->capacity != 0u && h->next >= h->capacity) { h->next = 0u; h->resets++; }
+    }
+  }
 }
 
 // Last view whose first tile is <= tile (binary search; warp-uniform).
@@ -116,8 +139,8 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
     traceViewsK(const stratum_view* __restrict__ V, int n, int grab, int order, BatchScratch* S) {
-  __shared__ StagedFeat feats[THREADS / 32][kKeys * kKeyStride];
-  __shared__ ChunkBox boxes[THREADS / 32][kKeys * (32 / kRun)];
+  __shared__ StagedFeat feats[THREADS / 32][32];
+  __shared__ ChunkBox boxes[THREADS / 32][32 / kRun];
   const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
   const int total = int(S->counters[kTotalTiles]);
 #pragma unroll 1
@@ -142,7 +165,7 @@ __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
                                1.08f / float(H));
 #else
       TraceResult r = traceWarp(V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2, cam.pos, rd,
-                                1.08f / float(H), inFrame, feats[warp], boxes[warp]);
+                                1.08f / float(H), inFrame, feats[warp], boxes[warp], groupCache(V[v].Groups));
       if (!inFrame) continue;
 #endif
       storeTrace(V[v].Hit, V[v].Surface, size_t(y) * W + x, r);
@@ -216,7 +239,10 @@ int render(stratum_view* V, int n, void* scratch, unsigned long long bytes, cons
   stratum_tune t = tune ? *tune : stratum_tune{128, 1, 1};
   if (!tuneOk(t)) return STRATUM_EINVAL;
   BatchScratch* S = static_cast<BatchScratch*>(scratch);
-  if (parts & kTrace) prologueK<<<1, 256, 0, s>>>(V, n, t.order, S);
+  if (parts & kTrace) {
+    cacheResetK<<<dim3(64, n), 256, 0, s>>>(V, n);
+    prologueK<<<1, 256, 0, s>>>(V, n, t.order, S);
+  }
   if (t.threads == 64) return launchParts<64>(V, n, t, S, s, parts);
   if (t.threads == 256) return launchParts<256>(V, n, t, S, s, parts);
   return launchParts<128>(V, n, t, S, s, parts);
@@ -266,6 +292,15 @@ int stratumHierarchyGrid();
 extern "C" {
 
 unsigned long long stratum_batchScratchBytes(int views) { return views > 0 ? batchScratchBytes(views) : 0; }
+
+unsigned long long stratum_groupCacheBytes(int entries) { return entries >= 0 ? groupCacheBytes(entries) : 0; }
+int stratum_groupCacheInit(unsigned* Groups, int entries, stratum_stream_t stream) {
+  if (!Groups || entries < 0) return STRATUM_EINVAL;
+  cudaError_t e = cudaMemsetAsync(Groups, 0, kCacheEntryOffset, asStream(stream));
+  if (e != cudaSuccess) return -int(e);
+  cacheInitK<<<1, 1, 0, asStream(stream)>>>(Groups, uint32_t(entries));
+  return launchStatus();
+}
 
 int stratum_applyPoses(stratum_view* views, const stratum_pose* poses, const int* flags, int n,
                        stratum_stream_t stream) {

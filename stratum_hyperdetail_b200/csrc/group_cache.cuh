@@ -1,0 +1,154 @@
+// Group cache: a per-table, lazily filled store of the feature records of the
+// (lot, group) pairs that rays evaluate, so that a group's records are built by
+// the grammar once and then loaded, instead of rebuilt every time a warp needs
+// them.  A frame evaluates each distinct group hundreds of times (one 1600x900
+// frame: 10^5-10^6 group evaluations over 10^3-10^5 distinct groups).
+//
+// Layout of one cache buffer (stratum_groupCacheBytes):
+//   header   256 B   next free entry, capacity (entries), resets, fills
+//   dir      16,384 x 64 u32: per (slot, group) 0 = empty, kCacheBusy = being
+//            filled, else entry index + 1
+//   entries  capacity x 1,856 B: a 64-byte tag (the lot descriptor words the
+//            grammar reads, the group, the count) and 56 records of 32 bytes
+//
+// An entry serves a (slot, group) only while its tag equals the slot's current
+// descriptor words and the group, so a table refreshed by any path (batched or
+// the drop-in prepareLots) never reads a stale entry: a mismatch is a miss.
+// Records are written once per entry and published by a release store of the
+// directory word after every lane's stores and a fence; readers take the
+// directory word with an acquire load.  A warp that finds a group being filled
+// by another warp, or the store full, builds the records with the grammar
+// itself and does not wait.  When the store is full at the start of a frame,
+// the directory is cleared and filling starts again.
+#pragma once
+#include "grammar_ra.cuh"
+
+namespace st {
+
+struct alignas(16) StagedFeat {
+  float px, py, pz, hx;
+  float hy, hz;
+  int packed;  // shape + 1 | material << 8 | turn << 16
+  float seed;
+};
+SD void stage(StagedFeat& s, const Feat& f) {
+  s.px = f.p.x; s.py = f.p.y; s.pz = f.p.z; s.hx = f.h.x; s.hy = f.h.y; s.hz = f.h.z;
+  s.packed = (f.shape + 1) | (f.material << 8) | (f.turn << 16);
+  s.seed = f.seed;
+}
+SD Feat unstage(const StagedFeat& s) {
+  return Feat{mk(s.px, s.py, s.pz), mk(s.hx, s.hy, s.hz), (s.packed & 255) - 1, (s.packed >> 8) & 255,
+              (s.packed >> 16) & 255, s.seed};
+}
+
+struct GroupCacheHeader {
+  uint32_t next, capacity, resets, fills;
+  uint32_t pad[60];
+};
+static_assert(sizeof(GroupCacheHeader) == 256, "group cache header is 256 bytes");
+constexpr uint32_t kCacheBusy = 0xFFFFFFFFu;
+constexpr int kCacheDirWords = kLots * kGroups;
+constexpr int kEntryRecords = 56;  // the largest group (group 30 of a building lot)
+constexpr int kEntryTagWords = 16;  // 64 bytes, 11 used
+constexpr size_t kEntryBytes = size_t(kEntryTagWords) * 4 + size_t(kEntryRecords) * sizeof(StagedFeat);
+constexpr size_t kCacheDirOffset = sizeof(GroupCacheHeader);
+constexpr size_t kCacheEntryOffset = kCacheDirOffset + size_t(kCacheDirWords) * 4;
+static_assert(kEntryBytes % 16 == 0 && kCacheEntryOffset % 16 == 0, "entries are 16-byte aligned");
+
+inline size_t groupCacheBytes(int entries) { return kCacheEntryOffset + size_t(entries > 0 ? entries : 0) * kEntryBytes; }
+
+struct GroupCache {
+  GroupCacheHeader* hdr;
+  uint32_t* dir;
+  char* entries;
+  uint32_t capacity;  // 0: no cache
+};
+SD GroupCache groupCache(uint32_t* base) {
+  GroupCache c;
+  c.hdr = reinterpret_cast<GroupCacheHeader*>(base);
+  c.dir = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(base) + kCacheDirOffset);
+  c.entries = reinterpret_cast<char*>(base) + kCacheEntryOffset;
+  c.capacity = base ? c.hdr->capacity : 0u;
+  return c;
+}
+SD uint32_t* entryTag(const GroupCache& c, uint32_t e) {
+  return reinterpret_cast<uint32_t*>(c.entries + size_t(e) * kEntryBytes);
+}
+SD StagedFeat* entryRecords(const GroupCache& c, uint32_t e) {
+  return reinterpret_cast<StagedFeat*>(c.entries + size_t(e) * kEntryBytes + kEntryTagWords * 4);
+}
+
+SD uint32_t loadAcquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+SD void storeRelease(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Tag word k of (descriptor row, group, count): the nine descriptor words the
+// grammar reads (w, d, h, type, material, floors, seed, storey, roofScale),
+// then the group and the record count.
+SD uint32_t tagWord(const float* row, int group, int count, int k) {
+  if (k < 9) return __float_as_uint(__ldg(row + k));
+  if (k == 9) return uint32_t(group);
+  if (k == 10) return uint32_t(count);
+  return 0u;
+}
+
+// Warp-collective: the entry holding (slot, group) with this descriptor, or -1.
+// Every lane of the warp calls it with the same arguments.
+SD int cacheFind(const GroupCache& c, const float* W, int slot, int group, int count) {
+  if (c.capacity == 0u) return -1;
+  const int lane = int(threadIdx.x & 31);
+  const uint32_t d = loadAcquire(c.dir + slot * kGroups + group);
+  if (d == 0u || d == kCacheBusy || d > c.capacity) return -1;
+  const uint32_t e = d - 1u;
+  bool same = true;
+  if (lane < kEntryTagWords)
+    same = __ldcg(entryTag(c, e) + lane) == tagWord(W + size_t(slot) * kLotFloats, group, count, lane);
+  return __all_sync(0xffffffffu, same) ? int(e) : -1;
+}
+
+// Warp-collective: claim a fresh entry for (slot, group), or -1 when another
+// warp is filling it or the store is full.  A claimed entry must be published.
+SD int cacheClaim(const GroupCache& c, int slot, int group) {
+  if (c.capacity == 0u) return -1;
+  int e = -1;
+  if ((threadIdx.x & 31) == 0) {
+    uint32_t* dp = c.dir + slot * kGroups + group;
+    const uint32_t old = loadAcquire(dp);
+    if (old != kCacheBusy && atomicCAS(dp, old, kCacheBusy) == old) {
+      const uint32_t i = atomicAdd(&c.hdr->next, 1u);
+      if (i < c.capacity) e = int(i);
+      else atomicExch(dp, old);  // full: leave the word as it was
+    }
+  }
+  return __shfl_sync(0xffffffffu, e, 0);
+}
+
+// Warp-collective: publish a claimed entry whose records the lanes have written.
+SD void cachePublish(const GroupCache& c, const float* W, int slot, int group, int count, int e) {
+  const int lane = int(threadIdx.x & 31);
+  if (lane < kEntryTagWords) entryTag(c, uint32_t(e))[lane] = tagWord(W + size_t(slot) * kLotFloats, group, count, lane);
+  __threadfence();
+  __syncwarp();
+  if (lane == 0) {
+    storeRelease(c.dir + slot * kGroups + group, uint32_t(e) + 1u);
+    atomicAdd(&c.hdr->fills, 1u);
+  }
+}
+
+// Record i of a found entry (a plain load through L2: the entry was published
+// before the acquire that found it, or by an earlier kernel).
+SD StagedFeat cacheRecord(const GroupCache& c, int e, int i) {
+  const float4* p = reinterpret_cast<const float4*>(entryRecords(c, uint32_t(e)) + i);
+  const float4 a = __ldcg(p), b = __ldcg(p + 1);
+  StagedFeat s;
+  s.px = a.x; s.py = a.y; s.pz = a.z; s.hx = a.w;
+  s.hy = b.x; s.hz = b.y; s.packed = __float_as_int(b.z); s.seed = b.w;
+  return s;
+}
+
+}  // namespace st

@@ -2,8 +2,9 @@
 //
 // A session is one camera in one seeded world at one resolution.  While it is
 // resident its whole device state lives in one allocation: descriptor table,
-// tags, the 64 MiB hierarchy, refresh queue, camera state and frame buffers
-// including the 64-sample accumulation buffer.  Moving or revisiting therefore
+// tags, the 64 MiB hierarchy, the table's group cache, refresh queue, camera
+// state and frame buffers including the 64-sample accumulation buffer.  The
+// group cache is not snapshotted on eviction: it refills as the session renders.  Moving or revisiting therefore
 // refreshes only the lots whose address changed (prepareLots' tag compare).
 //
 // Admission is by an HBM budget: a session is admitted when its bytes fit;
@@ -47,8 +48,9 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Byte offsets of one session's buffers inside its single allocation.
 struct Layout {
-  size_t C, Origin, I, World, Tags, Nodes, Queue, Hit, Surface, Linear, History, Pixels, total;
-  static Layout of(int w, int h) {
+  size_t C, Origin, I, World, Tags, Nodes, Queue, Hit, Surface, Linear, History, Pixels, Groups, total;
+  int groupEntries;
+  static Layout of(int w, int h, int groupEntries) {
     Layout L{};
     size_t o = 0, P = size_t(w) * size_t(h);
     auto take = [&](size_t bytes) { size_t at = o; o += align256(bytes); return at; };
@@ -57,6 +59,8 @@ struct Layout {
     L.Queue = take(size_t(kLots + 1) * 4);
     L.Hit = take(P * 16); L.Surface = take(P * 16); L.Linear = take(P * 16); L.History = take(P * 16);
     L.Pixels = take(P * 4);
+    L.groupEntries = groupEntries;
+    L.Groups = groupEntries > 0 ? take(stratum_groupCacheBytes(groupEntries)) : 0;
     L.total = o;
     return L;
   }
@@ -92,6 +96,7 @@ struct Session {
     v.World = at<float>(lay.World); v.Tags = at<unsigned>(lay.Tags); v.Nodes = at<float>(lay.Nodes);
     v.Queue = at<unsigned>(lay.Queue); v.Hit = at<float>(lay.Hit); v.Surface = at<float>(lay.Surface);
     v.Linear = at<float>(lay.Linear); v.History = at<float>(lay.History); v.Pixels = at<unsigned>(lay.Pixels);
+    v.Groups = lay.groupEntries > 0 ? at<unsigned>(lay.Groups) : nullptr;
     v.width = width; v.height = height; v.dt = 0.0f;
     return v;
   }
@@ -120,6 +125,7 @@ struct stratum_server {
   int device = 0;
   unsigned long long budget = 0;
   int maxViews = 1;
+  int groupEntries = 65536;
   stratum_tune tune{64, 1, 1};
   std::mutex mu;
   std::condition_variable cv;
@@ -202,6 +208,9 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
   if (st == STRATUM_OK)
     st = stratum_initCamera(s.at<float>(s.lay.C), s.at<unsigned>(s.lay.Origin), s.seed,
                             reinterpret_cast<stratum_stream_t>(S->admitStream));
+  if (st == STRATUM_OK && s.lay.groupEntries > 0)
+    st = stratum_groupCacheInit(s.at<unsigned>(s.lay.Groups), s.lay.groupEntries,
+                                reinterpret_cast<stratum_stream_t>(S->admitStream));
   if (st == STRATUM_OK && s.hasSnap) {  // continue exactly where the session left
     size_t P = size_t(s.width) * size_t(s.height);
     e = cudaMemcpyAsync(s.at<float>(s.lay.C), s.snapC.data(), 64 * 4, cudaMemcpyHostToDevice, S->admitStream);
@@ -397,6 +406,14 @@ stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_v
   return raw;
 }
 
+int stratum_server_set_group_cache(stratum_server* S, int entries) {
+  if (!S || entries < 0) return STRATUM_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (!S->sessions.empty()) return STRATUM_EINVAL;
+  S->groupEntries = entries;
+  return STRATUM_OK;
+}
+
 void stratum_server_destroy(stratum_server* S) {
   if (!S) return;
   S->stop.store(true);
@@ -427,7 +444,7 @@ int stratum_server_open(stratum_server* S, int seed, int width, int height, int*
   s->seed = seed;
   s->width = width;
   s->height = height;
-  s->lay = Layout::of(width, height);
+  s->lay = Layout::of(width, height, S->groupEntries);
   *session = s->id;
   S->sessions[s->id] = std::move(s);
   return STRATUM_OK;

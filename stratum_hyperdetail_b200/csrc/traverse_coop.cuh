@@ -7,9 +7,11 @@
 //    the lot's hierarchy -- until it reaches a leaf (a group) that must be
 //    evaluated, or finishes;
 //  * the warp then evaluates pending leaves one distinct (lot, group) key at a
-//    time: all 32 lanes build the group's features in shared memory, one
-//    feature per lane (random-access grammar, grammar_ra.cuh), and every lane
-//    waiting on that key tests them in index order with one inlined
+//    time: the group's records are staged in shared memory, one per lane --
+//    loaded from the table's group cache (group_cache.cuh) when it holds the
+//    group, else built by the random-access grammar (grammar_ra.cuh) and, when
+//    the cache has room, stored there for every later evaluation -- and every
+//    lane waiting on that key tests them in index order with one inlined
 //    intersection routine and its precomputed inverse directions;
 //  * the winner's normal, material and seed are recomputed once per ray.
 //
@@ -20,46 +22,14 @@
 #pragma once
 #include "geometry.cuh"
 #include "grammar_ra.cuh"
+#include "group_cache.cuh"
 #include "traverse.cuh"
 
 namespace st {
 
 // featureAt out of line: one copy, away from the hot test loop in the
 // instruction cache (measured faster than inlining it).
-#ifndef STRATUM_FEATUREAT_INLINE
 static __device__ __noinline__ Feat featureAtOOL(LotDesc L, int g, int i) { return featureAt(L, g, i); }
-#define ST_FEATURE_AT featureAtOOL
-#else
-#define ST_FEATURE_AT featureAt
-#endif
-
-// A feature staged in shared memory: two 16-byte words; shape (+1), material
-// and turn packed into one (shape >= -1, material and turn in [0, 255]).
-struct alignas(16) StagedFeat {
-  float px, py, pz, hx;
-  float hy, hz;
-  int packed;
-  float seed;
-};
-SD void stage(StagedFeat& s, const Feat& f) {
-  s.px = f.p.x; s.py = f.p.y; s.pz = f.p.z; s.hx = f.h.x; s.hy = f.h.y; s.hz = f.h.z;
-  s.packed = (f.shape + 1) | (f.material << 8) | (f.turn << 16);
-  s.seed = f.seed;
-}
-SD Feat unstage(const StagedFeat& s) {
-  return Feat{mk(s.px, s.py, s.pz), mk(s.hx, s.hy, s.hz), (s.packed & 255) - 1, (s.packed >> 8) & 255,
-              (s.packed >> 16) & 255, s.seed};
-}
-// Keys (distinct lot, group pairs) a warp evaluates at once, and the staged
-// stride per key: 33 records, so the same record index of different keys falls
-// in different shared-memory banks.  One key at a time measured fastest on the
-// benchmark poses (2 and 4 keys: 9 % and 19 % slower): staging several keys
-// costs more than the extra lanes it keeps busy.
-#ifndef STRATUM_COOP_KEYS
-#define STRATUM_COOP_KEYS 1
-#endif
-constexpr int kKeys = STRATUM_COOP_KEYS;
-constexpr int kKeyStride = 33;
 
 // Sub-group culling: every run of kRun staged features gets a box (in the
 // lot frame) that contains every point where any of them can be hit, and a
@@ -193,13 +163,33 @@ SD float coopHit(const Feat& f, const CoopRay& r) {
   return featureHitCore(f, r.lr, r.ld, intoFeature(r.lr - f.p, f.turn), d, odd ? r.inv1 : r.inv0, r.cone);
 }
 
+// The winner's record for one lane: from the group cache when it holds the
+// group, else from the grammar.
+SD Feat winnerFeature(const GroupCache& c, const float* __restrict__ W, int slot, int g, int i) {
+  const LotDesc L = loadLot(W, slot);
+  if (c.capacity != 0u) {
+    const uint32_t d = loadAcquire(c.dir + slot * kGroups + g);
+    if (d != 0u && d != kCacheBusy && d <= c.capacity) {
+      const int count = groupCount(L, g);
+      const uint4* tp = reinterpret_cast<const uint4*>(entryTag(c, d - 1u));
+      const uint4 a = __ldcg(tp), b = __ldcg(tp + 1), e = __ldcg(tp + 2);
+      const float* row = W + size_t(slot) * kLotFloats;
+      const uint32_t got[11] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x, e.y, e.z};
+      bool same = true;
+#pragma unroll
+      for (int k = 0; k < 11; k++) same = same && got[k] == tagWord(row, g, count, k);
+      if (same) return unstage(cacheRecord(c, int(d - 1u), i));
+    }
+  }
+  return featureAtOOL(L, g, i);
+}
+
 // The whole warp traces its 32 rays.  Every lane of the warp must call this
-// (inactive lanes with active = false).  `feats` = kKeys * kKeyStride staged
-// records and
-// `boxes` = kKeys * 32 / kRun chunk boxes of this warp, in shared memory
-// (staged records at key * kKeyStride).
+// (inactive lanes with active = false).  `feats` (32 records) and `boxes`
+// (32 / kRun chunk boxes) are this warp's shared-memory staging area; `cache`
+// is the table's group cache (capacity 0: none).
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
-                         f3 rd, float cone, bool active, StagedFeat* feats, ChunkBox* boxes) {
+                         f3 rd, float cone, bool active, StagedFeat* feats, ChunkBox* boxes, const GroupCache& cache) {
   const int lane = int(threadIdx.x & 31);
   CoopRay r;
   coopBegin(r, ro, rd, cone, active);
@@ -210,72 +200,55 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
     if (!pending) break;  // every lane is done (lanes only stop advancing at a leaf or when done)
 #pragma unroll 1
     while (pending) {
-      // Take up to kKeys distinct keys among the pending lanes.
-      const int key = (r.slot << 6) | r.pend;
-      int keys[kKeys];
-      unsigned batch = 0u;
-      int myq = -1;
-#pragma unroll
-      for (int q = 0; q < kKeys; q++) {
-        keys[q] = -1;
-        const unsigned rem = pending & ~batch;
-        if (rem) {
-          const int kq = __shfl_sync(0xffffffffu, key, __ffs(rem) - 1);
-          const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && key == kq);
-          keys[q] = kq;
-          batch |= peers;
-          if ((peers >> lane) & 1u) myq = q;
-        }
-      }
-      int myCount = 0, maxCount = 0;
-#pragma unroll
-      for (int q = 0; q < kKeys; q++)
-        if (keys[q] >= 0) {
-          const int c = groupCount(loadLot(W, keys[q] >> 6), keys[q] & 63);
-          if (myq == q) myCount = c;
-          maxCount = max(maxCount, c);
-        }
-      const int g = r.pend;
+      // the first pending lane's key, and every lane waiting on the same key
+      const int myKey = (r.slot << 6) | r.pend;
+      const int key = __shfl_sync(0xffffffffu, myKey, __ffs(pending) - 1);
+      const bool mine = r.state == kLeafPending && myKey == key;
+      const unsigned batch = __ballot_sync(0xffffffffu, mine);
+      const int slot = key >> 6, g = key & 63;
+      const LotDesc L = loadLot(W, slot);
+      const int count = groupCount(L, g);
+      int e = cacheFind(cache, W, slot, g, count);
+      const bool cached = e >= 0;
+      if (!cached) e = cacheClaim(cache, slot, g);  // -1: build without storing
 #pragma unroll 1
-      for (int base = 0; base < maxCount; base += 32) {
-        // stage, key by key: lane j builds feature base+j of the key and its
-        // hit box; runs of kRun lanes reduce their boxes into one chunk box
-#pragma unroll
-        for (int q = 0; q < kKeys; q++) {
-          if (keys[q] < 0) break;
-          const LotDesc L = loadLot(W, keys[q] >> 6);
-          const int gq = keys[q] & 63, count = groupCount(L, gq), j = base + lane;
-          f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
-          if (j < count) {
-            const Feat f = ST_FEATURE_AT(L, gq, j);
-            stage(feats[q * kKeyStride + lane], f);
-            hitBox(f, lo, hi);
+      for (int base = 0; base < count; base += 32) {
+        // stage: lane j holds record base+j and its hit box; runs of kRun
+        // lanes reduce their boxes into one chunk box
+        const int j = base + lane;
+        f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
+        if (j < count) {
+          StagedFeat s;
+          if (cached) {
+            s = cacheRecord(cache, e, j);
+          } else {
+            stage(s, featureAtOOL(L, g, j));
+            if (e >= 0) entryRecords(cache, uint32_t(e))[j] = s;
           }
-#pragma unroll
-          for (int o = 1; o < kRun; o <<= 1) {
-            lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
-                             __shfl_xor_sync(0xffffffffu, lo.z, o)));
-            hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
-                             __shfl_xor_sync(0xffffffffu, hi.z, o)));
-          }
-          if ((lane & (kRun - 1)) == 0)
-            boxes[q * (32 / kRun) + lane / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
+          feats[lane] = s;
+          hitBox(unstage(s), lo, hi);
         }
+#pragma unroll
+        for (int o = 1; o < kRun; o <<= 1) {
+          lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
+                           __shfl_xor_sync(0xffffffffu, lo.z, o)));
+          hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
+                           __shfl_xor_sync(0xffffffffu, hi.z, o)));
+        }
+        if ((lane & (kRun - 1)) == 0) boxes[lane / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
         __syncwarp();
-        // every waiting lane tests its own key's staged features
-        if (myq >= 0 && base < myCount) {
-          const StagedFeat* fq = feats + myq * kKeyStride;
-          const ChunkBox* bq = boxes + myq * (32 / kRun);
-          const int m = min(32, myCount - base);
+        // every waiting lane tests the staged records
+        if (mine) {
+          const int m = min(32, count - base);
 #pragma unroll 1
           for (int c = 0; c * kRun < m; c++) {
-            const ChunkBox b = bq[c];
+            const ChunkBox b = boxes[c];
             const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
             if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
             const int kEnd = min(m, (c + 1) * kRun);
 #pragma unroll 1
             for (int k = c * kRun; k < kEnd; k++) {
-              const Feat f = unstage(fq[k]);
+              const Feat f = unstage(feats[k]);
               const bool odd = f.turn % 2 == 1;
               const f3 inv = odd ? r.inv1 : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
               const Span rg = featureSlab(f, p, inv);
@@ -290,7 +263,8 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
         }
         __syncwarp();
       }
-      if (myq >= 0) { r.state = kInLot; r.node = popNode(r.stack); }
+      if (!cached && e >= 0) cachePublish(cache, W, slot, g, count, e);
+      if (mine) { r.state = kInLot; r.node = popNode(r.stack); }
       pending &= ~batch;
     }
   }
@@ -299,7 +273,7 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
   out.normal = mk(0.0f, 1.0f, 0.0f);
   if (r.fid >= 0) {  // the winner's record, lot frame and normal (trace.cu:53-54)
     const LotDesc L = loadLot(W, r.wslot);
-    const Feat f = featureAt(L, r.fid >> 6, r.fid & 63);
+    const Feat f = winnerFeature(cache, W, r.wslot, r.fid >> 6, r.fid & 63);
     f3 cp = mk(float(r.wcx) * kCell + L.ox, 0.0f, float(r.wcz) * kCell + L.oz);
     f3 lr = toLot(ro - cp, L.turn), ld = toLot(rd, L.turn);
     out.normal = fromLot(featureNormal(f, lr + ld * r.best), L.turn);

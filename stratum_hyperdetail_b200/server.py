@@ -65,19 +65,25 @@ def _lib():
         L.stratum_server_stats_get.argtypes = [vp, ct.POINTER(Stats)]
         L.stratum_server_inject.argtypes = [vp, ct.c_int, ct.c_int]
         L.stratum_server_read.argtypes = [vp, ct.c_int, vp, vp]
-        for n in ("open", "close", "submit", "wait", "stats_get", "inject", "read"):
+        L.stratum_server_set_group_cache.argtypes = [vp, ct.c_int]
+        for n in ("open", "close", "submit", "wait", "stats_get", "inject", "read", "set_group_cache"):
             getattr(L, "stratum_server_" + n).restype = ct.c_int
         _typed = True
     return L
 
 
 class Server:
-    def __init__(self, budget_bytes: int, max_views: int = 16, streams: int = 3, tune=(64, 1, 1)):
+    def __init__(self, budget_bytes: int, max_views: int = 16, streams: int = 3, tune=(64, 1, 1),
+                 group_cache: int | None = None):
+        """`group_cache`: group cache entries per session (None: the library's
+        default of 65,536; 0: none)."""
         self.L = _lib()
         t = Tune(*tune)
         self.h = self.L.stratum_server_create(int(budget_bytes), int(max_views), int(streams), ct.byref(t))
         if not self.h:
             raise RuntimeError("stratum_server_create failed")
+        if group_cache is not None and self.L.stratum_server_set_group_cache(self.h, int(group_cache)) != 0:
+            raise ValueError("bad group cache size")
         self.sizes = {}
 
     def close(self):

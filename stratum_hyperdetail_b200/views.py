@@ -11,7 +11,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from . import BUILD_CHUNKS, GROUP_NODES, LOT_FLOATS, WORLD_LOTS, call, ptr
+from . import BUILD_CHUNKS, GROUP_CACHE_ENTRIES, GROUP_NODES, LOT_FLOATS, WORLD_LOTS, call, lib, ptr
 
 ROWS = 64
 
@@ -33,12 +33,25 @@ class View:
         self.Hit, self.Surface = z(P * 4, f32), z(P * 4, f32)
         self.Linear, self.History = z(P * 4, f32), z(P * 4, f32)
         self.Pixels = z(P, i32)
+        self.Groups = None  # group cache of the table (batched trace only)
 
     @property
     def nbytes(self) -> int:
         return sum(t.numel() * t.element_size() for t in (self.C, self.Origin, self.I, self.World, self.Tags,
                                                           self.Nodes, self.Queue, self.Args, self.Hit, self.Surface,
-                                                          self.Linear, self.History, self.Pixels))
+                                                          self.Linear, self.History, self.Pixels)) + (
+            0 if self.Groups is None else self.Groups.numel() * 4)
+
+    def enable_group_cache(self, entries: int = GROUP_CACHE_ENTRIES, stream=None):
+        """Give the table a group cache of `entries` groups (read and filled by
+        the batched trace; results are the same with or without it).  0
+        removes it."""
+        if entries <= 0:
+            self.Groups = None
+            return
+        n = int(lib().stratum_groupCacheBytes(int(entries)))
+        self.Groups = torch.empty((n + 3) // 4, dtype=torch.int32, device=self.World.device)
+        call("stratum_groupCacheInit", ptr(self.Groups), int(entries), _s(stream))
 
     def set_pose(self, seed, origin, pos, yaw, pitch, shadows=True, stream=None):
         """initCamera(seed), place the camera in the lot frame of `origin`,

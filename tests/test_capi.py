@@ -37,9 +37,9 @@ def test_library_exports_every_declared_symbol():
 
 def test_python_signatures_cover_header():
     import stratum_hyperdetail_b200 as sb
-    # the two non-status functions are typed separately in lib(); the server's in server.py
+    # the three non-status functions are typed separately in lib(); the server's in server.py
     names = {n for n in declared_symbols() if not n.startswith("stratum_server_")}
-    assert names - {"stratum_version", "stratum_batchScratchBytes"} <= set(sb.SIGNATURES)
+    assert names - {"stratum_version", "stratum_batchScratchBytes", "stratum_groupCacheBytes"} <= set(sb.SIGNATURES)
     from stratum_hyperdetail_b200 import server
     L = server._lib()
     for n in declared_symbols():

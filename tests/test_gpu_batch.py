@@ -96,3 +96,62 @@ def test_autotune_picks_a_valid_tune_and_keeps_state(cuda):
     torch.cuda.synchronize()
     for i, v in enumerate(views):
         assert_same(snapshot(v), want[i], f"after autotune view {i}")
+
+
+def cache_header(v):
+    """(next, capacity, resets, fills) of a view's group cache."""
+    return tuple(int(x) for x in v.Groups[:4].cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.parametrize("entries", [0, 4, 65536])
+def test_group_cache_size_does_not_change_results(cuda, entries):
+    """No cache, a 4-group cache (full at once: most groups built by the
+    grammar, emptied at every frame) and the default cache give the plain
+    path's bits."""
+    from stratum_hyperdetail_b200.batch import Batch
+    want = plain_frames(3)
+    views = make_views()
+    b = Batch(views, (128, 1, 1), group_cache=entries)
+    for f in range(3):
+        b.frame()
+        torch.cuda.synchronize()
+        for i, v in enumerate(views):
+            assert_same(snapshot(v), want[f][i], f"cache {entries} frame {f} view {i}")
+    for v in views:
+        if entries == 0:
+            assert v.Groups is None
+            continue
+        nxt, cap, resets, fills = cache_header(v)
+        assert cap == entries and fills > 0
+        if entries == 4:
+            assert resets >= 2
+        else:
+            assert resets == 0 and nxt == fills  # everything fits; no group filled twice per slot change
+
+
+def test_group_cache_survives_a_table_moved_by_the_drop_in_path(cuda):
+    """A warm cache whose table is then re-described by the single-view entry
+    points (set_pose at another address) must not serve stale groups."""
+    from stratum_hyperdetail_b200.batch import Batch
+    views = make_views()
+    b = Batch(views, (128, 1, 1))
+    b.frame()
+    torch.cuda.synchronize()
+    # same seeds (the table is keyed by address), origins moved by a few lots:
+    # some slots keep their lots and cached groups, the others are re-described
+    moved = [(s, [o[0] + 3, o[1], o[2] ^ 5, o[3]], p, y, t, w, h) for s, o, p, y, t, w, h in VIEWS]
+    from stratum_hyperdetail_b200.views import View
+    fresh = []
+    for v, (seed, origin, pos, yaw, pitch, w, h) in zip(views, moved):
+        v.set_pose(seed, origin, pos, yaw, pitch)
+        v.History.zero_()
+        f = View(w, h)
+        f.set_pose(seed, origin, pos, yaw, pitch)
+        fresh.append(f)
+    b.frame()
+    for f in fresh:
+        f.frame(0.0)
+    torch.cuda.synchronize()
+    for i, (v, f) in enumerate(zip(views, fresh)):
+        for k in ("Hit", "Surface", "Linear", "Pixels"):
+            assert torch.equal(getattr(v, k), getattr(f, k)), f"view {i} {k} differs after the move"

@@ -84,8 +84,11 @@ def test_eviction_and_readmission_continue_exactly(cuda):
     sizes = [(160, 90), (128, 72), (144, 81)]
     poses = [poses_for(i, 6, origin=(i * 77, 0, 3 * i, 0)) for i in range(3)]
     want = [run_alone(50 + i, *sizes[i], poses[i]) for i in range(3)]
-    one = 66 * MB + max(w * h for w, h in sizes) * 68 + 4 * MB
-    srv = Server(2 * one, max_views=2, streams=2)  # room for two sessions: the third evicts
+    import stratum_hyperdetail_b200 as sb
+    cache = int(sb.lib().stratum_groupCacheBytes(4096))
+    one = 66 * MB + max(w * h for w, h in sizes) * 68 + 4 * MB + cache
+    # room for two sessions: the third evicts (the group cache is not kept)
+    srv = Server(2 * one, max_views=2, streams=2, group_cache=4096)
     sids = [srv.open(50 + i, *sizes[i]) for i in range(3)]
     for k in range(6):
         for i in range(3):
@@ -101,8 +104,8 @@ def test_eviction_and_readmission_continue_exactly(cuda):
 
 def test_budget_refusal_and_injected_allocation_failure(cuda):
     from stratum_hyperdetail_b200.server import BUDGET_EXCEEDED, Pose, Server
-    srv = Server(150 * MB, max_views=2, streams=1)
-    big = srv.open(1, 1920, 1080)  # needs ~197 MiB: never fits
+    srv = Server(150 * MB, max_views=2, streams=1, group_cache=1024)
+    big = srv.open(1, 1920, 1080)  # needs ~203 MiB: never fits
     small = srv.open(2, 96, 54)
     p = Pose.make((0, 0, 0, 0), (14.0, 1.7, 14.0), 0.0, 0.0)
     assert srv.wait_status(srv.submit(big, p)) == BUDGET_EXCEEDED
