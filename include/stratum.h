@@ -157,7 +157,9 @@ typedef struct stratum_view {
  * records (1,856 bytes each) plus a 4 MiB directory.  Entries are checked
  * against the table's current descriptor rows, so the cache never needs
  * invalidating when the table is refreshed (by any entry point); a full cache
- * is emptied at the start of the next batched frame.  Results are identical
+ * is emptied at the start of the next batched frame.  A trace launch uses the
+ * groups filled by earlier launches (the first frame of a view fills, the
+ * following ones reuse; at most 16,777,214 entries).  Results are identical
  * with and without a cache.  Initialise once before use (zeroes the directory,
  * sets the capacity); a zero-filled buffer is a cache of capacity 0. */
 unsigned long long stratum_groupCacheBytes(int entries);

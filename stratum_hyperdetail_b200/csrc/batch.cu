@@ -71,15 +71,15 @@ __global__ void __launch_bounds__(64) buildViewsK(const stratum_view* __restrict
 __global__ void cacheResetK(const stratum_view* __restrict__ V, int n) {
   const int v = int(blockIdx.y);
   if (v >= n || !V[v].Groups) return;
-  const GroupCache c = groupCache(V[v].Groups);
-  if (c.capacity == 0u || c.hdr->next < c.capacity) return;
-  uint4* d = reinterpret_cast<uint4*>(c.dir);
+  const GroupCacheHeader* h = reinterpret_cast<const GroupCacheHeader*>(V[v].Groups);
+  if (h->capacity == 0u || h->next < h->capacity) return;
+  uint4* d = reinterpret_cast<uint4*>(groupCache(V[v].Groups).dir(0, 0));
   for (int i = int(blockIdx.x * blockDim.x + threadIdx.x); i < kCacheDirWords / 4; i += int(gridDim.x * blockDim.x))
     d[i] = make_uint4(0u, 0u, 0u, 0u);
 }
 __global__ void cacheInitK(uint32_t* base, uint32_t entries) {
   GroupCacheHeader* h = reinterpret_cast<GroupCacheHeader*>(base);
-  h->next = 0u; h->capacity = entries; h->resets = 0u; h->fills = 0u;
+  h->next = 0u; h->capacity = entries; h->resets = 0u; h->fills = 0u; h->launches = 0u;
 }
 
 __global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
@@ -99,6 +99,7 @@ __global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
     if (V[v].Groups) {  // after cacheResetK: a full cache starts again
       GroupCacheHeader* h = reinterpret_cast<GroupCacheHeader*>(V[v].Groups);
       if (h->capacity != 0u && h->next >= h->capacity) { h->next = 0u; h->resets++; }
+      h->launches++;  // this launch's epoch
     }
   }
 }
@@ -295,7 +296,7 @@ unsigned long long stratum_batchScratchBytes(int views) { return views > 0 ? bat
 
 unsigned long long stratum_groupCacheBytes(int entries) { return entries >= 0 ? groupCacheBytes(entries) : 0; }
 int stratum_groupCacheInit(unsigned* Groups, int entries, stratum_stream_t stream) {
-  if (!Groups || entries < 0) return STRATUM_EINVAL;
+  if (!Groups || entries < 0 || uint32_t(entries) > kCacheMaxEntries) return STRATUM_EINVAL;
   cudaError_t e = cudaMemsetAsync(Groups, 0, kCacheEntryOffset, asStream(stream));
   if (e != cudaSuccess) return -int(e);
   cacheInitK<<<1, 1, 0, asStream(stream)>>>(Groups, uint32_t(entries));

@@ -5,21 +5,25 @@
 // frame: 10^5-10^6 group evaluations over 10^3-10^5 distinct groups).
 //
 // Layout of one cache buffer (stratum_groupCacheBytes):
-//   header   256 B   next free entry, capacity (entries), resets, fills
+//   header   256 B   next free entry, capacity (entries), resets, fills,
+//                    trace launches
 //   dir      16,384 x 64 u32: per (slot, group) 0 = empty, kCacheBusy = being
-//            filled, else entry index + 1
+//            filled, else (launch epoch << 24) | (entry index + 1)
 //   entries  capacity x 1,856 B: a 64-byte tag (the lot descriptor words the
 //            grammar reads, the group, the count) and 56 records of 32 bytes
 //
 // An entry serves a (slot, group) only while its tag equals the slot's current
 // descriptor words and the group, so a table refreshed by any path (batched or
 // the drop-in prepareLots) never reads a stale entry: a mismatch is a miss.
-// Records are written once per entry and published by a release store of the
-// directory word after every lane's stores and a fence; readers take the
-// directory word with an acquire load.  A warp that finds a group being filled
-// by another warp, or the store full, builds the records with the grammar
-// itself and does not wait.  When the store is full at the start of a frame,
-// the directory is cleared and filling starts again.
+// Each trace launch has an epoch (its launch count, 8 bits).  A launch reads
+// only entries filled by earlier launches: the kernel boundary makes them
+// visible, so plain (even read-only-path) loads are correct and no acquire is
+// needed.  Entries filled in the current launch are misses for that launch.  A
+// warp that misses claims the group (one atomic compare-and-swap on its
+// directory word) and fills an entry, or, when another warp holds it or the
+// store is full, builds the records with the grammar itself: nothing waits.
+// When the store is full at the start of a launch, the directory is cleared
+// and filling starts again.
 #pragma once
 #include "grammar_ra.cuh"
 
@@ -42,11 +46,12 @@ SD Feat unstage(const StagedFeat& s) {
 }
 
 struct GroupCacheHeader {
-  uint32_t next, capacity, resets, fills;
-  uint32_t pad[60];
+  uint32_t next, capacity, resets, fills, launches;
+  uint32_t pad[59];
 };
 static_assert(sizeof(GroupCacheHeader) == 256, "group cache header is 256 bytes");
 constexpr uint32_t kCacheBusy = 0xFFFFFFFFu;
+constexpr uint32_t kCacheMaxEntries = (1u << 24) - 2u;  // entry index + 1 fits 24 bits and is never 0xFFFFFF
 constexpr int kCacheDirWords = kLots * kGroups;
 constexpr int kEntryRecords = 56;  // the largest group (group 30 of a building lot)
 constexpr int kEntryTagWords = 16;  // 64 bytes, 11 used
@@ -57,34 +62,31 @@ static_assert(kEntryBytes % 16 == 0 && kCacheEntryOffset % 16 == 0, "entries are
 
 inline size_t groupCacheBytes(int entries) { return kCacheEntryOffset + size_t(entries > 0 ? entries : 0) * kEntryBytes; }
 
+// A cache is its base address alone (kept in two registers through the
+// traversal); capacity and epoch are read from the header when needed.  Those
+// two header words do not change during a trace launch (the prologue before it
+// writes them), so the read-only path may cache them.
 struct GroupCache {
-  GroupCacheHeader* hdr;
-  uint32_t* dir;
-  char* entries;
-  uint32_t capacity;  // 0: no cache
+  uint32_t* base;  // null: no cache
+  SD GroupCacheHeader* hdr() const { return reinterpret_cast<GroupCacheHeader*>(base); }
+  SD uint32_t capacity() const { return base ? __ldg(base + 1) : 0u; }
+  SD uint32_t epoch() const { return __ldg(base + 4) & 255u; }
+  SD uint32_t* dir(int slot, int group) const {
+    return reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(base) + kCacheDirOffset) + slot * kGroups + group;
+  }
+  SD char* entry(uint32_t e) const { return reinterpret_cast<char*>(base) + kCacheEntryOffset + size_t(e) * kEntryBytes; }
 };
-SD GroupCache groupCache(uint32_t* base) {
-  GroupCache c;
-  c.hdr = reinterpret_cast<GroupCacheHeader*>(base);
-  c.dir = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(base) + kCacheDirOffset);
-  c.entries = reinterpret_cast<char*>(base) + kCacheEntryOffset;
-  c.capacity = base ? c.hdr->capacity : 0u;
-  return c;
-}
-SD uint32_t* entryTag(const GroupCache& c, uint32_t e) {
-  return reinterpret_cast<uint32_t*>(c.entries + size_t(e) * kEntryBytes);
-}
+SD GroupCache groupCache(uint32_t* base) { return GroupCache{base}; }
+SD uint32_t* entryTag(const GroupCache& c, uint32_t e) { return reinterpret_cast<uint32_t*>(c.entry(e)); }
 SD StagedFeat* entryRecords(const GroupCache& c, uint32_t e) {
-  return reinterpret_cast<StagedFeat*>(c.entries + size_t(e) * kEntryBytes + kEntryTagWords * 4);
+  return reinterpret_cast<StagedFeat*>(c.entry(e) + kEntryTagWords * 4);
 }
 
-SD uint32_t loadAcquire(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-SD void storeRelease(uint32_t* p, uint32_t v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// The entry a directory word names if it was filled by an earlier launch, else -1.
+SD int usableEntry(const GroupCache& c, uint32_t d) {
+  if (d == 0u || d == kCacheBusy || (d >> 24) == c.epoch()) return -1;
+  const uint32_t e = (d & 0xFFFFFFu) - 1u;
+  return e < c.capacity() ? int(e) : -1;
 }
 
 // Tag word k of (descriptor row, group, count): the nine descriptor words the
@@ -99,52 +101,52 @@ SD uint32_t tagWord(const float* row, int group, int count, int k) {
 
 // Warp-collective: the entry holding (slot, group) with this descriptor, or -1.
 // Every lane of the warp calls it with the same arguments.
-SD int cacheFind(const GroupCache& c, const float* W, int slot, int group, int count) {
-  if (c.capacity == 0u) return -1;
+SD int cacheFind(const GroupCache& c, const float* W, int slot, int group, int count, uint32_t& word) {
+  word = 0u;
+  if (!c.base) return -1;
   const int lane = int(threadIdx.x & 31);
-  const uint32_t d = loadAcquire(c.dir + slot * kGroups + group);
-  if (d == 0u || d == kCacheBusy || d > c.capacity) return -1;
-  const uint32_t e = d - 1u;
+  word = __ldcg(c.dir(slot, group));
+  const int e = usableEntry(c, word);
+  if (e < 0) return -1;
   bool same = true;
   if (lane < kEntryTagWords)
-    same = __ldcg(entryTag(c, e) + lane) == tagWord(W + size_t(slot) * kLotFloats, group, count, lane);
-  return __all_sync(0xffffffffu, same) ? int(e) : -1;
+    same = __ldg(entryTag(c, uint32_t(e)) + lane) == tagWord(W + size_t(slot) * kLotFloats, group, count, lane);
+  return __all_sync(0xffffffffu, same) ? e : -1;
 }
 
 // Warp-collective: claim a fresh entry for (slot, group), or -1 when another
-// warp is filling it or the store is full.  A claimed entry must be published.
-SD int cacheClaim(const GroupCache& c, int slot, int group) {
-  if (c.capacity == 0u) return -1;
+// warp is filling it, filled it in this launch, or the store is full.  `old`
+// is the directory word cacheFind saw.  A claimed entry must be published.
+SD int cacheClaim(const GroupCache& c, int slot, int group, uint32_t old) {
+  if (c.capacity() == 0u || old == kCacheBusy || (old != 0u && (old >> 24) == c.epoch())) return -1;
   int e = -1;
   if ((threadIdx.x & 31) == 0) {
-    uint32_t* dp = c.dir + slot * kGroups + group;
-    const uint32_t old = loadAcquire(dp);
-    if (old != kCacheBusy && atomicCAS(dp, old, kCacheBusy) == old) {
-      const uint32_t i = atomicAdd(&c.hdr->next, 1u);
-      if (i < c.capacity) e = int(i);
+    uint32_t* dp = c.dir(slot, group);
+    if (atomicCAS(dp, old, kCacheBusy) == old) {
+      const uint32_t i = atomicAdd(&c.hdr()->next, 1u);
+      if (i < c.capacity()) e = int(i);
       else atomicExch(dp, old);  // full: leave the word as it was
     }
   }
   return __shfl_sync(0xffffffffu, e, 0);
 }
 
-// Warp-collective: publish a claimed entry whose records the lanes have written.
+// Warp-collective: publish a claimed entry whose records the lanes have
+// written.  Readers use it from the next launch on.
 SD void cachePublish(const GroupCache& c, const float* W, int slot, int group, int count, int e) {
   const int lane = int(threadIdx.x & 31);
   if (lane < kEntryTagWords) entryTag(c, uint32_t(e))[lane] = tagWord(W + size_t(slot) * kLotFloats, group, count, lane);
-  __threadfence();
   __syncwarp();
   if (lane == 0) {
-    storeRelease(c.dir + slot * kGroups + group, uint32_t(e) + 1u);
-    atomicAdd(&c.hdr->fills, 1u);
+    atomicExch(c.dir(slot, group), (c.epoch() << 24) | (uint32_t(e) + 1u));
+    atomicAdd(&c.hdr()->fills, 1u);
   }
 }
 
-// Record i of a found entry (a plain load through L2: the entry was published
-// before the acquire that found it, or by an earlier kernel).
+// Record i of a usable entry (filled by an earlier launch: read-only here).
 SD StagedFeat cacheRecord(const GroupCache& c, int e, int i) {
   const float4* p = reinterpret_cast<const float4*>(entryRecords(c, uint32_t(e)) + i);
-  const float4 a = __ldcg(p), b = __ldcg(p + 1);
+  const float4 a = __ldg(p), b = __ldg(p + 1);
   StagedFeat s;
   s.px = a.x; s.py = a.y; s.pz = a.z; s.hx = a.w;
   s.hy = b.x; s.hz = b.y; s.packed = __float_as_int(b.z); s.seed = b.w;

@@ -167,19 +167,15 @@ SD float coopHit(const Feat& f, const CoopRay& r) {
 // group, else from the grammar.
 SD Feat winnerFeature(const GroupCache& c, const float* __restrict__ W, int slot, int g, int i) {
   const LotDesc L = loadLot(W, slot);
-  if (c.capacity != 0u) {
-    const uint32_t d = loadAcquire(c.dir + slot * kGroups + g);
-    if (d != 0u && d != kCacheBusy && d <= c.capacity) {
-      const int count = groupCount(L, g);
-      const uint4* tp = reinterpret_cast<const uint4*>(entryTag(c, d - 1u));
-      const uint4 a = __ldcg(tp), b = __ldcg(tp + 1), e = __ldcg(tp + 2);
-      const float* row = W + size_t(slot) * kLotFloats;
-      const uint32_t got[11] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, e.x, e.y, e.z};
-      bool same = true;
-#pragma unroll
-      for (int k = 0; k < 11; k++) same = same && got[k] == tagWord(row, g, count, k);
-      if (same) return unstage(cacheRecord(c, int(d - 1u), i));
-    }
+  const int e = c.base ? usableEntry(c, __ldcg(c.dir(slot, g))) : -1;
+  if (e >= 0) {
+    const int count = groupCount(L, g);
+    const uint32_t* tag = entryTag(c, uint32_t(e));
+    const float* row = W + size_t(slot) * kLotFloats;
+    bool same = true;
+#pragma unroll 1
+    for (int k = 0; k < 11 && same; k++) same = __ldg(tag + k) == tagWord(row, g, count, k);
+    if (same) return unstage(cacheRecord(c, e, i));
   }
   return featureAtOOL(L, g, i);
 }
@@ -187,7 +183,7 @@ SD Feat winnerFeature(const GroupCache& c, const float* __restrict__ W, int slot
 // The whole warp traces its 32 rays.  Every lane of the warp must call this
 // (inactive lanes with active = false).  `feats` (32 records) and `boxes`
 // (32 / kRun chunk boxes) are this warp's shared-memory staging area; `cache`
-// is the table's group cache (capacity 0: none).
+// is the table's group cache (null base or capacity 0: none).
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
                          f3 rd, float cone, bool active, StagedFeat* feats, ChunkBox* boxes, const GroupCache& cache) {
   const int lane = int(threadIdx.x & 31);
@@ -208,9 +204,10 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
       const int slot = key >> 6, g = key & 63;
       const LotDesc L = loadLot(W, slot);
       const int count = groupCount(L, g);
-      int e = cacheFind(cache, W, slot, g, count);
+      uint32_t word;
+      int e = cacheFind(cache, W, slot, g, count, word);
       const bool cached = e >= 0;
-      if (!cached) e = cacheClaim(cache, slot, g);  // -1: build without storing
+      if (!cached) e = cacheClaim(cache, slot, g, word);  // -1: build without storing
 #pragma unroll 1
       for (int base = 0; base < count; base += 32) {
         // stage: lane j holds record base+j and its hit box; runs of kRun
