@@ -20,6 +20,14 @@ no data-path collective; the reported time is the max over ranks.
 `--impl reference` times the reference's own renderer (its kernels compiled as
 host C++, oracle/_ref) on the host cores with every thread, on a bounded
 sample of the same workload (a 48-row band of each pose per step).
+
+Besides the headline, the line carries (N=1 only): the plain drop-in path on
+the same views, per-pose trace rates of both paths, serving runs (Poisson
+arrivals over resident sessions, p50/p99 latency; one with a budget small
+enough to evict), the batched multi-view scenario (`random_views`: 64 random
+views of uneven size, pose, seed and sample count) and the streaming flight
+(`streaming`: 1024x576 at 40 m/s across the 64-bit carry with periodic
+hierarchy-vs-exhaustive checks of 65,536 random rays).
 """
 from __future__ import annotations
 
@@ -82,8 +90,17 @@ def parse(argv=None):
     ap.add_argument("--poses", default=",".join(POSES), help="comma-separated subset of the six poses (profiling)")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of each serving run (0: skip)")
     ap.add_argument("--serve-views", type=int, default=8, help="views per serving batch")
+    ap.add_argument("--tune", default=None, help="threads,grab,order of the batched trace (default: autotune)")
+    ap.add_argument("--random-views", type=int, default=64, help="views of the random multi-view scenario (0: skip)")
+    ap.add_argument("--streaming-frames", type=int, default=1000, help="frames of the streaming flight (0: skip)")
+    ap.add_argument("--streaming-check-every", type=int, default=10,
+                    help="frames between hierarchy-vs-exhaustive checks of 65,536 random rays")
     a = ap.parse_args(argv)
     a.poses = [p for p in a.poses.split(",") if p]
+    if a.tune:
+        a.tune = tuple(int(x) for x in a.tune.split(","))
+        if len(a.tune) != 3:
+            ap.error("--tune wants threads,grab,order")
     unknown = set(a.poses) - set(POSES)
     if unknown:
         ap.error(f"unknown poses {sorted(unknown)}")
@@ -106,21 +123,63 @@ def init_dist(world):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled every 10 ms during
+    the timed region, read through NVML (read-only queries); nvidia-smi at its
+    200 ms minimum period when NVML is unavailable."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.lines = []
+        self.nvml = None
+        self.samples = []  # (sm_mhz, max_mhz, set of reason names)
+        self.stop = threading.Event()
+        self.thread = None
+        self.source = None
+
+    def _handle(self, nv):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            return nv.nvmlDeviceGetHandleByPciBusId(f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nvml, h = nv, self._handle(nv)
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+
+            def poll():
+                while True:
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((sm, mx, {n for n, b in bits.items() if r & b}))
+                    except Exception:
+                        pass
+                    if self.stop.wait(0.01):
+                        break
+            self.source = "nvml, 10 ms"
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi, 200 ms"
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -129,9 +188,23 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                self.samples.append((float(p[1]), float(p[2]),
+                                     {n for n, v in zip(self.NAMES, p[5:9]) if v.lower() == "active"}))
+            except ValueError:
+                continue
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml and self.thread:
+            self.thread.join(timeout=2)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -140,22 +213,167 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            p = [x.strip() for x in ln.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx = float(p[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [s[0] for s in self.samples]
+        reasons = set().union(*[s[2] for s in self.samples]) if self.samples else set()
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": self.samples[-1][1] if self.samples else None, "reasons": sorted(reasons),
+                "samples": len(sm), "source": self.source}
+
+
+def random_views(n_views, tune, steps=1, warmup=1):
+    """Batched multi-view scenario: `n_views` independent views drawn from a
+    counter-based PRNG (Philox) seeded 1 -- 16:9 with width log-uniform in
+    [320, 1920], lot address uniform over the 64-bit range per axis, altitude
+    uniform in 1.5-300 m, yaw uniform in [0, 360) deg, pitch uniform in [-45, 10]
+    deg, world seed uniform in [0, 2^24) (exact as the f32 camera word), and a
+    sample count uniform in 1-64.  A step renders every view's samples from the
+    start of its sequence: frame k draws sample k of the views that have at
+    least k samples (views sorted by count, so frame k is one batched call over
+    a prefix of the view table).  Separately, the fused build of all views' full
+    16,384-lot tables and hierarchies is timed (one refresh + one build launch)."""
+    import ctypes
+
+    import torch
+    import stratum_hyperdetail_b200 as sb
+    from stratum_hyperdetail_b200.batch import Batch
+    from stratum_hyperdetail_b200.views import View
+    rng = np.random.Generator(np.random.Philox(1))
+    specs = []
+    for _ in range(n_views):
+        w = int(round(320 * 6 ** rng.random()))
+        h = int(round(w * 9 / 16))
+        origin = [int(x) for x in rng.integers(0, 2**32, size=4, dtype=np.uint64)]
+        pos = (float(rng.uniform(-18, 18)), float(rng.uniform(1.5, 300.0)), float(rng.uniform(-18, 18)))
+        yaw, pitch = math.radians(rng.uniform(0, 360)), math.radians(rng.uniform(-45, 10))
+        seed, samples = int(rng.integers(0, 1 << 24)), int(rng.integers(1, 65))
+        specs.append((samples, w, h, seed, origin, pos, yaw, pitch))
+    specs.sort(key=lambda s: -s[0])
+    views = []
+    for samples, w, h, seed, origin, pos, yaw, pitch in specs:
+        v = View(w, h)
+        v.set_pose(seed, origin, pos, yaw, pitch)
+        views.append(v)
+    b = Batch(views, tune)
+    counts = [s[0] for s in specs]
+    prefix = [sum(1 for c in counts if c >= k) for k in range(1, max(counts) + 1)]
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+    poses = torch.zeros(n_views * 9, dtype=torch.float32, device="cuda")  # unused: pose flag bit 0 stays clear
+    restart = torch.full((n_views,), 2, dtype=torch.int32, device="cuda")
+    keep = torch.zeros(n_views, dtype=torch.int32, device="cuda")
+    args = (sb.ptr(b.table), sb.ptr(b.scratch), b.scratch_bytes)
+
+    def step():
+        sb.call("stratum_applyPoses", args[0], sb.ptr(poses), sb.ptr(restart), n_views, s)
+        for k, m in enumerate(prefix):
+            if k == 1:
+                sb.call("stratum_applyPoses", args[0], sb.ptr(poses), sb.ptr(keep), n_views, s)
+            sb.call("stratum_frameViews", args[0], m, args[1], args[2], ctypes.byref(b.tune), s)
+
+    for _ in range(warmup):
+        step()
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    ms = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        a, c = ev(), ev()
+        a.record(stream)
+        step()
+        c.record(stream)
+        c.synchronize()
+        ms.append(a.elapsed_time(c))
+    rays = sum(cnt * w * h for cnt, w, h, *_ in specs)
+    # fused full-table build of every view: invalidate the tables, then one refresh + one build launch
+    for v in views:
+        v.World.zero_()
+    torch.cuda.synchronize()
+    a, c = ev(), ev()
+    a.record(stream)
+    sb.call("stratum_refreshViews", args[0], n_views, s)
+    sb.call("stratum_buildViews", args[0], n_views, s)
+    c.record(stream)
+    c.synchronize()
+    build_ms = a.elapsed_time(c)
+    px = [w * h for _, w, h, *_ in specs]
+    out = {"views": n_views, "ray_samples_per_step": rays, "ms_per_step": float(np.mean(ms)),
+           "rays_per_s": rays / (float(np.mean(ms)) * 1e-3), "frames_per_step": len(prefix),
+           "mean_mpix_per_view": float(np.mean(px)) / 1e6, "mean_samples": float(np.mean(counts)),
+           "fused_build_ms": build_ms, "lots_built": n_views * 16384,
+           "gpu_launches_per_step": len(prefix) * b.launches_per_frame + (2 if len(prefix) > 1 else 1),
+           "tune": list(tune), "prng": "numpy Philox seeded 1"}
+    del b, views
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def streaming(frames, check_every, tune, rays_per_check=65536):
+    """Streaming-world scenario: one 1024x576 view flies straight along +x at
+    40 m/s and 40 m altitude, 60 Hz simulated time, from lot address
+    xl = 0xFFFFFFF0 (so the 64-bit carry into xh is crossed after 16 lots, at
+    frame 837).  Each frame is one batched frame call: stepCamera, refresh of the
+    lots that entered the 128x128 table (one 128-lot column per 36 m cell),
+    rebuild of their hierarchies, trace, shade and resolve.  Every
+    `check_every` frames, 65,536 uniformly random rays (Philox seeded 1: origins
+    uniform over the table's +-1 km square at 0.5-100 m, directions uniform on
+    the sphere) are traced through the hierarchy and exhaustively (every group
+    of every visited lot) and compared bit for bit; checks are outside the
+    frame timing."""
+    import torch
+    import stratum_hyperdetail_b200 as sb
+    from stratum_hyperdetail_b200.batch import Batch
+    from stratum_hyperdetail_b200.views import View
+    v = View(1024, 576)
+    v.set_pose(SEED, (0xFFFFFFF0, 0, 0, 0), (0.0, 40.0, 0.0), math.pi / 2, 0.0)
+    v.C[12] = 40.0
+    v.I[0] = 1.0
+    b = Batch([v], tune)
+    b.set_dt(1.0 / 60.0)
+    rng = np.random.Generator(np.random.Philox(1))
+    stream = torch.cuda.current_stream()
+    s = stream.cuda_stream
+    out_h = torch.empty(rays_per_check * 8, dtype=torch.float32, device="cuda")
+    out_e = torch.empty_like(out_h)
+    ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+    marks, checks, bad_t, bad_id, check_ms = [], 0, 0, 0, 0.0
+    for f in range(frames):
+        a, c = ev(), ev()
+        a.record(stream)
+        b.frame(stream)
+        c.record(stream)
+        marks.append((a, c))
+        if check_every and (f + 1) % check_every == 0:
+            n = rays_per_check
+            ro = np.stack([rng.uniform(-1000, 1000, n), rng.uniform(0.5, 100.0, n), rng.uniform(-1000, 1000, n)], 1)
+            d = rng.normal(size=(n, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            rays = torch.from_numpy(np.concatenate([ro, d, np.full((n, 1), 0.0015)], 1).astype(np.float32)).cuda()
+            x, y = ev(), ev()
+            x.record(stream)
+            sb.call("stratum_traceRays", sb.ptr(v.World), sb.ptr(v.Nodes), sb.ptr(v.Origin), sb.ptr(rays), n, 0,
+                    sb.ptr(out_h), s)
+            sb.call("stratum_traceRays", sb.ptr(v.World), sb.ptr(v.Nodes), sb.ptr(v.Origin), sb.ptr(rays), n, 1,
+                    sb.ptr(out_e), s)
+            y.record(stream)
+            y.synchronize()
+            check_ms += x.elapsed_time(y)
+            hb, eb = out_h.view(torch.int32).view(-1, 8), out_e.view(torch.int32).view(-1, 8)
+            bad_t += int((hb[:, 0] != eb[:, 0]).sum())
+            bad_id += int((hb[:, 1] != eb[:, 1]).sum())
+            checks += 1
+    torch.cuda.synchronize()
+    fm = np.array([a.elapsed_time(c) for a, c in marks])
+    org = v.Origin.cpu().numpy().view(np.uint32)
+    out = {"frames": frames, "width": 1024, "height": 576, "sim_distance_m": frames * 40.0 / 60.0,
+           "frame_ms_mean": float(fm.mean()), "frame_ms_p99": float(np.percentile(fm, 99)),
+           "frames_per_s": 1e3 / float(fm.mean()), "rays_per_s": 1024 * 576 / (float(fm.mean()) * 1e-3),
+           "final_origin": [int(x) for x in org], "carry_crossed": bool(org[1] == 1),
+           "checks": checks, "rays_checked": checks * rays_per_check, "distance_mismatches": bad_t,
+           "identity_mismatches": bad_id, "check_ms_mean": check_ms / max(checks, 1)}
+    del b, v
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
 
 
 # ---------------------------------------------------------------- CPU legs
@@ -364,11 +582,27 @@ def ours_arm(args):
     per_pose = {n: WIDTH * HEIGHT * args.steps / (trace_plain[i] * 1e-3) for i, n in enumerate(names)}
 
     # -- 2. the batched path: every view in one launch per kernel, autotuned
-    batch = Batch(views)
+    batch = Batch(views, args.tune or (128, 1, 1))
     batch.frame()
-    tune_ms = batch.autotune()
+    tune_ms = batch.autotune() if not args.tune else None
     tune = {"threads": batch.tune.threads, "grab": batch.tune.grab, "order": batch.tune.order,
-            "trace_ms": tune_ms}
+            "trace_ms": tune_ms, "source": "given" if args.tune else "autotune"}
+    tune_t = (batch.tune.threads, batch.tune.grab, batch.tune.order)
+    # per-pose trace rate of the batched kernel: each view alone in a batch (warm group cache)
+    per_pose_batched = {}
+    for name, v in zip(names, views):
+        one = Batch([v], tune_t)
+        one.trace(stream)
+        tt = []
+        for _ in range(3):
+            a, c = ev(), ev()
+            a.record(stream)
+            one.trace(stream)
+            c.record(stream)
+            c.synchronize()
+            tt.append(a.elapsed_time(c))
+        per_pose_batched[name] = WIDTH * HEIGHT / (min(tt) * 1e-3)
+        del one
     call, P, s = sb.call, sb.ptr, stream.cuda_stream
 
     def batch_step():
@@ -455,7 +689,6 @@ def ours_arm(args):
     # -- serving: continuous batching over resident sessions (open-loop Poisson arrivals)
     serving = None
     n_views = len(views)
-    tune_t = (batch.tune.threads, batch.tune.grab, batch.tune.order)
     batch.graph = None  # release the graph (and, below, the views) before serving and the process group
     del batch, views
     torch.cuda.synchronize()
@@ -466,8 +699,14 @@ def ours_arm(args):
                                                 args.serve_views, 3, tune_t),
             "sessions_64_at_1600x900": serve_poisson(200.0, 64, args.serve_seconds, (1600,), 150 << 30,
                                                      args.serve_views, 3, tune_t, seed=2),
+            # a budget that holds about two thirds of the sessions: LRU eviction and exact resumption at work
+            "mixed_256_sessions_40gb_budget": serve_poisson(200.0, 256, args.serve_seconds, (768, 1024, 1600, 1920),
+                                                            40 << 30, args.serve_views, 3, tune_t, seed=3),
             "plain_path_per_view_ms": sum(plain_ms) / args.steps / len(names),
         }
+    multi = random_views(args.random_views, tune_t) if args.random_views > 0 and world == 1 else None
+    stream_run = (streaming(args.streaming_frames, args.streaming_check_every, tune_t)
+                  if args.streaming_frames > 0 and world == 1 else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -497,11 +736,12 @@ def ours_arm(args):
                            "note": "reference launch structure: per view 15 trace + 15 shade strips of 64 rows"},
             "batched_eager": {"value": eager_value, "ms_per_step": sum(eager_ms) / args.steps},
             "batched_vs_plain": value / plain_value,
-            "per_pose_trace_rays_per_s": per_pose,
+            "per_pose_trace_rays_per_s": {"plain": per_pose, "batched": per_pose_batched},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "call": "stratum_frameViews over the batch, pinned host input and RGBA8 readback"},
-            "gpu_launches": launches, "clocks": clocks.summary(), "wall_s": wall, "serving": serving}
+            "gpu_launches": launches, "clocks": clocks.summary(), "wall_s": wall, "serving": serving,
+            "random_views": multi, "streaming": stream_run}
     if not graph_ok:
         line["graph_error"] = graph_err
     print(json.dumps(line), flush=True)

@@ -175,8 +175,13 @@ __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
   retire(&S->counters[kTraceNext], &S->counters[kTraceDone], THREADS);
 }
 
+// STRATUM_SHADE_OCC / THREADS resident blocks: 1536 threads per SM (40 registers,
+// some spills) measured fastest; shading is latency-bound.
+#ifndef STRATUM_SHADE_OCC
+#define STRATUM_SHADE_OCC 1536
+#endif
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) shadeViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
+__global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) shadeViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
                                                       BatchScratch* S) {
   const int lane = int(threadIdx.x & 31);
   const int total = int(S->counters[kTotalTiles]);

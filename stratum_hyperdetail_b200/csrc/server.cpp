@@ -86,7 +86,8 @@ struct Session {
   stratum_pose last{};
   double lastUse = 0.0;
   bool hasSnap = false;
-  std::vector<float> snapC, snapHist;
+  std::vector<float> snapC;
+  float* snapHist = nullptr;  // pinned: the accumulation buffer while evicted (kept for the next eviction)
   unsigned snapOrigin[4] = {0, 0, 0, 0};
   unsigned char* pinnedOut = nullptr;
   template <class T> T* at(size_t off) const { return reinterpret_cast<T*>(base + off); }
@@ -162,12 +163,15 @@ void finish(stratum_server* S, Request* r, int status) {
 int evict(stratum_server* S, Session& s) {
   size_t P = size_t(s.width) * size_t(s.height);
   s.snapC.resize(64);
-  s.snapHist.resize(P * 4);
+  if (!s.snapHist && cudaMallocHost(reinterpret_cast<void**>(&s.snapHist), P * 16) != cudaSuccess) {
+    s.snapHist = nullptr;
+    return -int(cudaGetLastError());
+  }
   cudaError_t e = cudaMemcpyAsync(s.snapC.data(), s.at<float>(s.lay.C), 64 * 4, cudaMemcpyDeviceToHost, S->admitStream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.snapOrigin, s.at<unsigned>(s.lay.Origin), 16, cudaMemcpyDeviceToHost, S->admitStream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.snapHist.data(), s.at<float>(s.lay.History), P * 16, cudaMemcpyDeviceToHost, S->admitStream);
+    e = cudaMemcpyAsync(s.snapHist, s.at<float>(s.lay.History), P * 16, cudaMemcpyDeviceToHost, S->admitStream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(S->admitStream);
   if (e != cudaSuccess) return -int(e);
   cudaFreeAsync(s.base, S->admitStream);
@@ -217,7 +221,7 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(s.at<unsigned>(s.lay.Origin), s.snapOrigin, 16, cudaMemcpyHostToDevice, S->admitStream);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s.at<float>(s.lay.History), s.snapHist.data(), P * 16, cudaMemcpyHostToDevice, S->admitStream);
+      e = cudaMemcpyAsync(s.at<float>(s.lay.History), s.snapHist, P * 16, cudaMemcpyHostToDevice, S->admitStream);
     if (e != cudaSuccess) st = -int(e);
   }
   if (st == STRATUM_OK && !s.pinnedOut) {
@@ -235,8 +239,6 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
   }
   s.resident = true;
   s.hasSnap = false;
-  s.snapHist.clear();
-  s.snapHist.shrink_to_fit();
   S->residentBytes += need;
   S->admissions++;
   return STRATUM_OK;
@@ -369,6 +371,8 @@ void freeSession(stratum_server* S, Session& s) {
   }
   if (s.pinnedOut) cudaFreeHost(s.pinnedOut);
   s.pinnedOut = nullptr;
+  if (s.snapHist) cudaFreeHost(s.snapHist);
+  s.snapHist = nullptr;
 }
 
 }  // namespace

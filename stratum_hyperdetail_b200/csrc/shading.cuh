@@ -8,21 +8,30 @@
 
 namespace st {
 
+// One out-of-line copy each of the value noise, the 5-octave fbm, the masonry
+// height field and powf for all shading call sites: inlined at every use they
+// multiply the kernel's code and it stalls on instruction fetch.  Same
+// arithmetic, same bits.
+static __device__ __noinline__ float noise2D(float x, float y) { return noise2(x, y); }
+static __device__ __noinline__ float fbm2D(float x, float y) { return fbm2(x, y); }
+static __device__ __noinline__ float masonryHeightD(float u, float v, int material) { return masonryHeight(u, v, material); }
+static __device__ __noinline__ float powD(float x, float y) { return powf(x, y); }
+
 SD f3 substrateMean(int m) { return m == 1 ? mk(0.37f, 0.185f, 0.105f) : mk(0.55f, 0.485f, 0.365f); }
 SD f3 substrate(float u, float v, float seed, int m) {
-  float large = fbm2(u * 0.31f + seed * 0.013f, v * 0.31f);
-  float run = fbm2(u * 0.42f + seed * 0.01f, v * 0.038f + 1.7f);
+  float large = fbm2D(u * 0.31f + seed * 0.013f, v * 0.31f);
+  float run = fbm2D(u * 0.42f + seed * 0.01f, v * 0.038f + 1.7f);
   f3 base = substrateMean(m);
   float age = 0.61f + 0.52f * large, damp = smooth(0.49f, 0.76f, run) * 0.31f;
   return base * (age - damp) + mk(0.017f, 0.024f, 0.014f) * damp;
 }
-SD f3 skyColor(f3 rd, f3 sun) {
+static __device__ __noinline__ f3 skyColor(f3 rd, f3 sun) {
   float elev = sat(rd.y);
-  f3 c = mix(mk(0.62f, 0.69f, 0.72f), mk(0.13f, 0.30f, 0.52f), powf(elev, 0.45f));
+  f3 c = mix(mk(0.62f, 0.69f, 0.72f), mk(0.13f, 0.30f, 0.52f), powD(elev, 0.45f));
   float sd = fmaxf(0.0f, dot(rd, sun));
-  c = c + mk(1.1f, 0.62f, 0.22f) * powf(sd, 18.0f) + mk(9.0f, 6.0f, 3.2f) * powf(sd, 2600.0f);
+  c = c + mk(1.1f, 0.62f, 0.22f) * powD(sd, 18.0f) + mk(9.0f, 6.0f, 3.2f) * powD(sd, 2600.0f);
   if (rd.y > 0.025f) {
-    float cloud = fbm2(rd.x / (rd.y + 0.20f) * 1.8f + 16.0f, rd.z / (rd.y + 0.20f) * 1.8f);
+    float cloud = fbm2D(rd.x / (rd.y + 0.20f) * 1.8f + 16.0f, rd.z / (rd.y + 0.20f) * 1.8f);
     float veil = smooth(0.46f, 0.70f, cloud) * smooth(0.02f, 0.2f, rd.y) * 0.55f;
     c = mix(c, mk(0.86f, 0.85f, 0.80f), veil);
   }
@@ -44,9 +53,9 @@ SD f3 mineralCell(float u, float v, int seed) {
   return mk(sqrtf(nearest), value, sqrtf(second) - sqrtf(nearest));
 }
 SD float microRelief(float u, float v, float fp) {
-  float value = (noise2(u * 83.0f, v * 83.0f) - 0.5f) * 0.0016f * freqWeight(fp, 83.0f);
-  value += (noise2(u * 277.0f + 8.7f, v * 277.0f) - 0.5f) * 0.00048f * freqWeight(fp, 277.0f);
-  value += (noise2(u * 911.0f, v * 911.0f - 13.9f) - 0.5f) * 0.00013f * freqWeight(fp, 911.0f);
+  float value = (noise2D(u * 83.0f, v * 83.0f) - 0.5f) * 0.0016f * freqWeight(fp, 83.0f);
+  value += (noise2D(u * 277.0f + 8.7f, v * 277.0f) - 0.5f) * 0.00048f * freqWeight(fp, 277.0f);
+  value += (noise2D(u * 911.0f, v * 911.0f - 13.9f) - 0.5f) * 0.00013f * freqWeight(fp, 911.0f);
   return value;
 }
 static __device__ __noinline__ f3 surfaceColor(f3 p, f3 n, int mat, float seed, float fp, f3 foundation) {
@@ -63,9 +72,9 @@ static __device__ __noinline__ f3 surfaceColor(f3 p, f3 n, int mat, float seed, 
     float variation = (hash2(brick, row, int(seed)) - 0.5f) * 0.19f * freqWeight(fp, 1.0f / bh);
     c = c * (1.0f + variation);
     c = mix(c, mk(0.25f, 0.245f, 0.21f), joint * 0.84f);
-    float pores = fine > 0.0f ? fbm2(u * 52.0f + seed, v * 52.0f) : 0.5f;
+    float pores = fine > 0.0f ? fbm2D(u * 52.0f + seed, v * 52.0f) : 0.5f;
     c = c * (1.0f + (pores - 0.5f) * 0.38f * fine);
-    float deposits = smooth(0.45f, 0.76f, fbm2(u * 5.1f + seed * 0.3f, v * 6.2f));
+    float deposits = smooth(0.45f, 0.76f, fbm2D(u * 5.1f + seed * 0.3f, v * 6.2f));
     c = mix(c, mk(0.52f, 0.49f, 0.39f), deposits * 0.23f * (1.0f - joint));
     if (fp < 0.007f) {
       f3 mineral = mineralCell(u * 190.0f, v * 190.0f, int(seed));
@@ -75,46 +84,46 @@ static __device__ __noinline__ f3 surfaceColor(f3 p, f3 n, int mat, float seed, 
       c = c * (1.0f - pit * 0.66f - grit * 0.075f);
       float fleck = (1.0f - smooth(0.04f, 0.17f, mineral.x)) * (1.0f - smooth(0.07f, 0.18f, mineral.y)) * detail;
       c = mix(c, mk(0.62f, 0.56f, 0.44f), fleck * 0.78f);
-      float powder = (noise2(u * 740.0f, v * 740.0f) - 0.5f) * freqWeight(fp, 740.0f);
+      float powder = (noise2D(u * 740.0f, v * 740.0f) - 0.5f) * freqWeight(fp, 740.0f);
       c = c * (1.0f + powder * (joint > 0.5f ? 0.50f : 0.24f));
     }
-    float crack = fabsf(sinf(u * 8.4f + fbm2(u * 2.4f, v * 2.4f) * 5.0f + v * 1.3f));
-    float fracture = (1.0f - smooth(0.012f, 0.042f + fp * 4.0f, crack)) * smooth(0.48f, 0.72f, noise2(u * 1.4f, v * 1.4f));
+    float crack = fabsf(sinf(u * 8.4f + fbm2D(u * 2.4f, v * 2.4f) * 5.0f + v * 1.3f));
+    float fracture = (1.0f - smooth(0.012f, 0.042f + fp * 4.0f, crack)) * smooth(0.48f, 0.72f, noise2D(u * 1.4f, v * 1.4f));
     c = c * (1.0f - fracture * 0.45f * freqWeight(fp, 15.0f));
-    float moss = (1.0f - smooth(0.1f, 3.1f, p.y)) * smooth(0.44f, 0.69f, noise2(u * 1.3f, v * 0.3f));
+    float moss = (1.0f - smooth(0.1f, 3.1f, p.y)) * smooth(0.44f, 0.69f, noise2D(u * 1.3f, v * 0.3f));
     c = mix(c, mk(0.095f, 0.125f, 0.046f), moss * 0.7f);
   } else if (mat == 2 || mat == 14) {  // slate / terracotta tiles
     c = mat == 2 ? mk(0.14f, 0.19f, 0.22f) : mk(0.38f, 0.125f, 0.048f);
     float tile = fract(u * 3.7f), row = fract(v * 4.4f);
     float seam = (1.0f - smooth(0.01f, 0.07f, tile)) + (1.0f - smooth(0.02f, 0.11f, row));
-    c = c * (0.78f + 0.26f * lerp(0.5f, noise2(u * 7.2f, v * 7.2f), freqWeight(fp, 7.2f)) -
+    c = c * (0.78f + 0.26f * lerp(0.5f, noise2D(u * 7.2f, v * 7.2f), freqWeight(fp, 7.2f)) -
              sat(seam) * 0.25f * freqWeight(fp, 4.4f));
   } else if (mat == 3) {  // copper patina
-    float patina = smooth(0.28f, 0.64f, fbm2(u * 2.1f, v * 2.1f));
+    float patina = smooth(0.28f, 0.64f, fbm2D(u * 2.1f, v * 2.1f));
     c = mix(mk(0.27f, 0.145f, 0.072f), mk(0.085f, 0.24f, 0.18f), patina);
     float seam = 1.0f - smooth(0.015f, 0.07f, fract(u * 1.8f));
     c = c * (1.0f - seam * 0.4f * freqWeight(fp, 1.8f));
   } else if (mat == 4) c = mk(0.045f, 0.084f, 0.093f);
   else if (mat == 5) {
-    float grain = sinf(u * 49.0f + fbm2(u * 2.0f, v * 0.5f) * 8.0f);
+    float grain = sinf(u * 49.0f + fbm2D(u * 2.0f, v * 0.5f) * 8.0f);
     c = mk(0.12f, 0.07f, 0.039f) * (1.0f + grain * 0.12f * fine);
-  } else if (mat == 6) c = mk(0.075f, 0.091f, 0.087f) * (0.8f + noise2(u * 30.0f, v * 30.0f) * 0.3f);
+  } else if (mat == 6) c = mk(0.075f, 0.091f, 0.087f) * (0.8f + noise2D(u * 30.0f, v * 30.0f) * 0.3f);
   else if (mat == 7) {
-    float leaves = fbm2(p.x * 8.0f + p.y * 6.0f, p.z * 8.0f);
+    float leaves = fbm2D(p.x * 8.0f + p.y * 6.0f, p.z * 8.0f);
     c = mix(mk(0.055f, 0.095f, 0.020f), mk(0.18f, 0.25f, 0.055f), leaves);
   } else if (mat == 8) c = mk(0.70f, 0.43f, 0.13f);
   else if (mat == 9) c = mk(0.035f, 0.115f, 0.12f);
   else if (mat == 10) {
-    float grit = lerp(0.5f, fbm2(u * 45.0f, v * 45.0f), freqWeight(fp, 45.0f));
+    float grit = lerp(0.5f, fbm2D(u * 45.0f, v * 45.0f), freqWeight(fp, 45.0f));
     c = mk(0.16f, 0.17f, 0.16f) * (0.72f + grit * 0.4f);
   } else if (mat == 11) {
     int row = int(floorf(v / 0.45f));
     float a = fract(u / 0.9f + float(imod(row, 2)) * 0.5f), b = fract(v / 0.45f);
     float joint = (1.0f - smooth(0.02f, 0.07f + fp, fminf(fminf(a, 1.0f - a), fminf(b, 1.0f - b))));
-    c = mk(0.43f, 0.415f, 0.36f) * (0.78f + fbm2(u * 18.0f, v * 18.0f) * 0.3f);
+    c = mk(0.43f, 0.415f, 0.36f) * (0.78f + fbm2D(u * 18.0f, v * 18.0f) * 0.3f);
     c = c * (1.0f - joint * 0.30f * freqWeight(fp, 2.0f));
-  } else if (mat == 13) c = mk(0.54f, 0.475f, 0.35f) * (0.82f + fbm2(u * 1.6f, v * 1.6f) * 0.24f);
-  else if (mat == 15) c = mk(0.17f, 0.12f, 0.065f) * (0.65f + 0.6f * fbm2(u * 31.0f, v * 3.0f));
+  } else if (mat == 13) c = mk(0.54f, 0.475f, 0.35f) * (0.82f + fbm2D(u * 1.6f, v * 1.6f) * 0.24f);
+  else if (mat == 15) c = mk(0.17f, 0.12f, 0.065f) * (0.65f + 0.6f * fbm2D(u * 31.0f, v * 3.0f));
   if (mat == 18) {
     float panel = fract(u / 1.6f);
     float frame = (1.0f - smooth(0.02f, 0.06f, panel)) + (1.0f - smooth(0.02f, 0.06f, 1.0f - panel));
@@ -209,8 +218,8 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
   const f3 ro = F.cam.pos, sun = F.sun;
   float t = hit.x;
   int id = int(hit.y);
-  f3 result = skyColor(rd, sun);
-  if (id == kSkyId) return result;
+  if (id == kSkyId) return skyColor(rd, sun);  // (a hit pixel's colour never reads the sky term)
+  f3 result;
   f3 p = ro + rd * t, n = mk(surf.x, surf.y, surf.z);
   int mat = int(hit.z), slot = int(surf.w);
   if (slot >= kLots) slot = -1;  // never index past the table on a malformed Surface
@@ -246,8 +255,8 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
   f3 originalN = n;
   if ((mat == 0 || mat == 1) && fabsf(qn.y) < 0.5f) {  // mortar relief normal by central differences
     float eps = fmaxf(0.002f, sfp * 0.6f);
-    float du = (masonryHeight(u + eps, v, mat) - masonryHeight(u - eps, v, mat)) / (2.0f * eps);
-    float dv = (masonryHeight(u, v + eps, mat) - masonryHeight(u, v - eps, mat)) / (2.0f * eps);
+    float du = (masonryHeightD(u + eps, v, mat) - masonryHeightD(u - eps, v, mat)) / (2.0f * eps);
+    float dv = (masonryHeightD(u, v + eps, mat) - masonryHeightD(u, v - eps, mat)) / (2.0f * eps);
     if (sfp < 0.005f) {
       float me = fmaxf(0.00016f, sfp * 0.8f);
       du += (microRelief(u + me, v, sfp) - microRelief(u - me, v, sfp)) / (2.0f * me);
@@ -274,7 +283,7 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
   float k = (rough + 1.0f) * (rough + 1.0f) / 8.0f;
   float geometry = nv / (nv * (1.0f - k) + k) * nl / (nl * (1.0f - k) + k + 0.00001f);
   float f0 = mat == 3 || mat == 6 || mat == 8 ? 0.35f : 0.045f;
-  float fresnel = f0 + (1.0f - f0) * powf(1.0f - vh, 5.0f);
+  float fresnel = f0 + (1.0f - f0) * powD(1.0f - vh, 5.0f);
   float spec = distribution * geometry * fresnel / (4.0f * nv * nl + 0.0001f);
   f3 direct = mk(2.25f, 1.72f, 1.18f) * (nl * shadow);
   float skyWeight = 0.22f + 0.29f * sat(n.y * 0.5f + 0.5f);
@@ -283,7 +292,7 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
   result = albedo * (direct + ambient) + mk(1.0f, 0.87f, 0.63f) * (spec * nl * shadow * 2.1f);
   if (mat == 4 || mat == 9) {
     f3 reflection = rd - n * (2.0f * dot(rd, n));
-    float fr = 0.10f + 0.72f * powf(1.0f - nv, 4.0f);
+    float fr = 0.10f + 0.72f * powD(1.0f - nv, 4.0f);
     result = mix(result, skyColor(reflection, sun) * 0.60f, fr);
     if (mat == 4) {
       float room = hash1(int(seed));
@@ -291,7 +300,7 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
     }
   }
   if (mat == 8) result = result + mk(1.1f, 0.62f, 0.19f) * 0.8f;
-  if (mat == 7) result = result + albedo * (powf(fmaxf(0.0f, dot(rd, sun)), 4.0f) * 0.35f);
+  if (mat == 7) result = result + albedo * (powD(fmaxf(0.0f, dot(rd, sun)), 4.0f) * 0.35f);
   float fog = 1.0f - expf(-t * 0.00068f);
   fog = lerp(fog, 1.0f, smooth(kFar * 0.68f, kFar, t));
   f3 haze = skyColor(unit(mk(rd.x, 0.004f, rd.z)), sun);
@@ -351,7 +360,7 @@ SD void resolvePixel(f3 c, float4* Hist, uint32_t* Px, const FrameConst& F, cons
   Hist[b] = make_float4(c.x, c.y, c.z, count);
   float sx = (float(x) / float(width) - 0.5f) * 1.3f, sy = (float(y) / float(height) - 0.5f) * 1.3f;
   c = c * (F.exposure * (1.0f - (sx * sx + sy * sy) * 0.12f));
-  c = mk(powf(aces(c.x), 1.0f / 2.2f), powf(aces(c.y), 1.0f / 2.2f), powf(aces(c.z), 1.0f / 2.2f));
+  c = mk(powD(aces(c.x), 1.0f / 2.2f), powD(aces(c.y), 1.0f / 2.2f), powD(aces(c.z), 1.0f / 2.2f));
   Px[b] = packRGBA8(c);
 }
 
