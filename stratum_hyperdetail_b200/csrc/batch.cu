@@ -140,8 +140,7 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
     traceViewsK(const stratum_view* __restrict__ V, int n, int grab, int order, BatchScratch* S) {
-  __shared__ StagedFeat feats[THREADS / 32][32];
-  __shared__ ChunkBox boxes[THREADS / 32][32 / kRun];
+  extern __shared__ __align__(16) unsigned char stageBytes[];  // THREADS / 32 WarpStage
   const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
   const int total = int(S->counters[kTotalTiles]);
 #pragma unroll 1
@@ -166,7 +165,8 @@ __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
                                1.08f / float(H));
 #else
       TraceResult r = traceWarp(V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2, cam.pos, rd,
-                                1.08f / float(H), inFrame, feats[warp], boxes[warp], groupCache(V[v].Groups));
+                                1.08f / float(H), inFrame, reinterpret_cast<WarpStage*>(stageBytes)[warp],
+                                groupCache(V[v].Groups));
       if (!inFrame) continue;
 #endif
       storeTrace(V[v].Hit, V[v].Surface, size_t(y) * W + x, r);
@@ -211,13 +211,16 @@ __global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) shadeVie
 }
 
 template <class K>
-int residentBlocks(K kernel, int threads) {
+int residentBlocks(K kernel, int threads, size_t smem = 0) {
   int dev = 0, sms = 148, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
   return sms * (per > 0 ? per : 1);
 }
+// Dynamic shared memory of a trace block: one WarpStage per warp.
+constexpr size_t traceSmem(int threads) { return size_t(threads / 32) * sizeof(WarpStage); }
 
 enum Parts { kTrace = 1, kShade = 2 };
 
@@ -225,10 +228,10 @@ template <int T>
 int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratch* S, cudaStream_t s, int parts) {
   static int traceGrid = 0, shadeGrid = 0;
   if (!traceGrid) {
-    traceGrid = residentBlocks(traceViewsK<T>, T);
+    traceGrid = residentBlocks(traceViewsK<T>, T, traceSmem(T));
     shadeGrid = residentBlocks(shadeViewsK<T>, T);
   }
-  if (parts & kTrace) traceViewsK<T><<<traceGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
+  if (parts & kTrace) traceViewsK<T><<<traceGrid, T, traceSmem(T), s>>>(V, n, t.grab, t.order, S);
   if (parts & kShade) shadeViewsK<T><<<shadeGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
   return launchStatus();
 }

@@ -180,12 +180,66 @@ SD Feat winnerFeature(const GroupCache& c, const float* __restrict__ W, int slot
   return featureAtOOL(L, g, i);
 }
 
+// Groups a warp stages and tests at once: lanes waiting on different groups
+// then test concurrently, each its own group's records.  One group at a time
+// measured fastest on the six benchmark poses (2, 3, 4 groups: frame 6 %, 16 %,
+// 27 % slower, the aerial view included), so the default is 1.
+#ifndef STRATUM_COOP_KEYS
+#define STRATUM_COOP_KEYS 1
+#endif
+constexpr int kKeys = STRATUM_COOP_KEYS;
+constexpr int kRunsPerGroup = (kEntryRecords + kRun - 1) / kRun;
+// Shared memory of one warp: kKeys groups of up to 56 records and their chunk boxes.
+struct WarpStage {
+  StagedFeat feats[kKeys][kEntryRecords];
+  ChunkBox boxes[kKeys][kRunsPerGroup];
+};
+
+// Stage one group into slot q of the warp's stage: its records from the group
+// cache, or built by the grammar (and stored when the cache gives an entry),
+// and the chunk boxes.  Warp-collective; returns the group's record count.
+SD int stageGroup(const float* __restrict__ W, const GroupCache& cache, int key, WarpStage& ws, int q) {
+  const int lane = int(threadIdx.x & 31);
+  const int slot = key >> 6, g = key & 63;
+  const LotDesc L = loadLot(W, slot);
+  const int count = groupCount(L, g);
+  uint32_t word;
+  int e = cacheFind(cache, W, slot, g, count, word);
+  const bool cached = e >= 0;
+  if (!cached) e = cacheClaim(cache, slot, g, word);  // -1: build without storing
+#pragma unroll 1
+  for (int base = 0; base < count; base += 32) {
+    const int j = base + lane;
+    f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
+    if (j < count) {
+      StagedFeat s;
+      if (cached) {
+        s = cacheRecord(cache, e, j);
+      } else {
+        stage(s, featureAtOOL(L, g, j));
+        if (e >= 0) entryRecords(cache, uint32_t(e))[j] = s;
+      }
+      ws.feats[q][j] = s;
+      hitBox(unstage(s), lo, hi);
+    }
+#pragma unroll
+    for (int o = 1; o < kRun; o <<= 1) {
+      lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
+                       __shfl_xor_sync(0xffffffffu, lo.z, o)));
+      hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
+                       __shfl_xor_sync(0xffffffffu, hi.z, o)));
+    }
+    if ((lane & (kRun - 1)) == 0 && j < count) ws.boxes[q][j / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
+  }
+  if (!cached && e >= 0) cachePublish(cache, W, slot, g, count, e);
+  return count;
+}
+
 // The whole warp traces its 32 rays.  Every lane of the warp must call this
-// (inactive lanes with active = false).  `feats` (32 records) and `boxes`
-// (32 / kRun chunk boxes) are this warp's shared-memory staging area; `cache`
-// is the table's group cache (null base or capacity 0: none).
+// (inactive lanes with active = false).  `ws` is this warp's shared-memory
+// staging area; `cache` is the table's group cache (null base: none).
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
-                         f3 rd, float cone, bool active, StagedFeat* feats, ChunkBox* boxes, const GroupCache& cache) {
+                         f3 rd, float cone, bool active, WarpStage& ws, const GroupCache& cache) {
   const int lane = int(threadIdx.x & 31);
   CoopRay r;
   coopBegin(r, ro, rd, cone, active);
@@ -194,74 +248,51 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
     coopAdvance(r, W, N, o0, o2);
     unsigned pending = __ballot_sync(0xffffffffu, r.state == kLeafPending);
     if (!pending) break;  // every lane is done (lanes only stop advancing at a leaf or when done)
+    const int myKey = (r.slot << 6) | r.pend;
 #pragma unroll 1
     while (pending) {
-      // the first pending lane's key, and every lane waiting on the same key
-      const int myKey = (r.slot << 6) | r.pend;
-      const int key = __shfl_sync(0xffffffffu, myKey, __ffs(pending) - 1);
-      const bool mine = r.state == kLeafPending && myKey == key;
-      const unsigned batch = __ballot_sync(0xffffffffu, mine);
-      const int slot = key >> 6, g = key & 63;
-      const LotDesc L = loadLot(W, slot);
-      const int count = groupCount(L, g);
-      uint32_t word;
-      int e = cacheFind(cache, W, slot, g, count, word);
-      const bool cached = e >= 0;
-      if (!cached) e = cacheClaim(cache, slot, g, word);  // -1: build without storing
-#pragma unroll 1
-      for (int base = 0; base < count; base += 32) {
-        // stage: lane j holds record base+j and its hit box; runs of kRun
-        // lanes reduce their boxes into one chunk box
-        const int j = base + lane;
-        f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
-        if (j < count) {
-          StagedFeat s;
-          if (cached) {
-            s = cacheRecord(cache, e, j);
-          } else {
-            stage(s, featureAtOOL(L, g, j));
-            if (e >= 0) entryRecords(cache, uint32_t(e))[j] = s;
-          }
-          feats[lane] = s;
-          hitBox(unstage(s), lo, hi);
-        }
+      // up to kKeys distinct keys of the pending lanes (first pending lane's
+      // key first), staged one after another
+      unsigned batch = 0u;
+      int myq = -1, myCount = 0;
 #pragma unroll
-        for (int o = 1; o < kRun; o <<= 1) {
-          lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
-                           __shfl_xor_sync(0xffffffffu, lo.z, o)));
-          hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
-                           __shfl_xor_sync(0xffffffffu, hi.z, o)));
-        }
-        if ((lane & (kRun - 1)) == 0) boxes[lane / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
-        __syncwarp();
-        // every waiting lane tests the staged records
-        if (mine) {
-          const int m = min(32, count - base);
+      for (int q = 0; q < kKeys; q++) {
+        const unsigned rem = pending & ~batch;
+        if (!rem) break;
+        const int key = __shfl_sync(0xffffffffu, myKey, __ffs(rem) - 1);
+        const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && myKey == key);
+        batch |= peers;
+        const int count = stageGroup(W, cache, key, ws, q);
+        if ((peers >> lane) & 1u) { myq = q; myCount = count; }
+      }
+      __syncwarp();
+      // every waiting lane tests its own group's records in index order
+      if (myq >= 0) {
+        const int g = r.pend;
 #pragma unroll 1
-          for (int c = 0; c * kRun < m; c++) {
-            const ChunkBox b = boxes[c];
-            const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
-            if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
-            const int kEnd = min(m, (c + 1) * kRun);
+        for (int c = 0; c * kRun < myCount; c++) {
+          const ChunkBox b = ws.boxes[myq][c];
+          const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
+          if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
+          const int kEnd = min(myCount, (c + 1) * kRun);
 #pragma unroll 1
-            for (int k = c * kRun; k < kEnd; k++) {
-              const Feat f = unstage(feats[k]);
-              const bool odd = f.turn % 2 == 1;
-              const f3 inv = odd ? r.inv1 : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
-              const Span rg = featureSlab(f, p, inv);
-              if (featureSlabMiss(f, rg)) continue;
-              const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
-              const float th = featureAfterSlab(f, r.lr, r.ld, p, d, inv, rg, r.cone);
-              if (th > 0.001f && th < r.best) {  // index order: the first feature wins ties
-                r.best = th; r.fid = g * kMaxFeatures + base + k; r.wslot = r.slot; r.wcx = r.lcx; r.wcz = r.lcz;
-              }
+          for (int k = c * kRun; k < kEnd; k++) {
+            const Feat f = unstage(ws.feats[myq][k]);
+            const bool odd = f.turn % 2 == 1;
+            const f3 inv = odd ? r.inv1 : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
+            const Span rg = featureSlab(f, p, inv);
+            if (featureSlabMiss(f, rg)) continue;
+            const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
+            const float th = featureAfterSlab(f, r.lr, r.ld, p, d, inv, rg, r.cone);
+            if (th > 0.001f && th < r.best) {  // index order: the first feature wins ties
+              r.best = th; r.fid = g * kMaxFeatures + k; r.wslot = r.slot; r.wcx = r.lcx; r.wcz = r.lcz;
             }
           }
         }
-        __syncwarp();
+        r.state = kInLot;
+        r.node = popNode(r.stack);
       }
-      if (!cached && e >= 0) cachePublish(cache, W, slot, g, count, e);
-      if (mine) { r.state = kInLot; r.node = popNode(r.stack); }
+      __syncwarp();
       pending &= ~batch;
     }
   }
