@@ -13,9 +13,13 @@
 //                   the resolve taps, computed once per frame
 //   traceViewsK     persistent: each warp claims `grab` 8x4-pixel tiles at a
 //                   time from a device queue over all views and traces them
-//   shadeViewsK     persistent: shade + resolve of the same tiles, fused
+//   shadeViewsK     persistent: shading of the same tiles (Linear)
+//   resolveViewsK   persistent: contact occlusion, accumulation and tone map
+//                   (History, Pixels); a kernel of its own because the two
+//                   fused measured slower (the shading code alone fills the
+//                   instruction cache)
 //
-// The two queues reset themselves: the last warp to find a queue empty zeroes
+// The tile queues reset themselves: the last warp to find a queue empty zeroes
 // its counters, so consecutive launches (and graph replays) need no memset.
 #include "batch.cuh"
 #include "common_api.cuh"
@@ -204,10 +208,37 @@ __global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) shadeVie
       const float4* surf = reinterpret_cast<const float4*>(V[v].Surface);
       f3 c = shadePixel(V[v].World, F, hit[b], surf[b], primaryDir(F.cam, x, y, W, H), H);
       reinterpret_cast<float4*>(V[v].Linear)[b] = make_float4(c.x, c.y, c.z, 1.0f);
-      resolvePixel(c, reinterpret_cast<float4*>(V[v].History), V[v].Pixels, F, S->taps, hit, surf, W, H, x, y);
     }
   }
   retire(&S->counters[kShadeNext], &S->counters[kShadeDone], THREADS);
+}
+
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) resolveViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
+                                                        BatchScratch* S) {
+  const int lane = int(threadIdx.x & 31);
+  const int total = int(S->counters[kTotalTiles]);
+#pragma unroll 1
+  for (;;) {
+    const int t0 = claim(&S->counters[kResolveNext], grab);
+    if (t0 >= total) break;
+    const int t1 = min(t0 + grab, total);
+#pragma unroll 1
+    for (int tile = t0; tile < t1; tile++) {
+      const int v = viewOf(V, n, tile);
+      const int W = V[v].width, H = V[v].height;
+      int tx, ty;
+      if (!tileCoord(tile - V[v].tileBase, V[v].tilesX, (H + kTileH - 1) / kTileH, order, tx, ty)) continue;
+      const int x = tx * kTileW + (lane & 7), y = ty * kTileH + (lane >> 3);
+      if (x >= W || y >= H) continue;
+      const FrameConst F = S->view[v];
+      const size_t b = size_t(y) * W + x;
+      const float4 l = reinterpret_cast<const float4*>(V[v].Linear)[b];
+      resolvePixel(mk(l.x, l.y, l.z), reinterpret_cast<float4*>(V[v].History), V[v].Pixels, F, S->taps,
+                   reinterpret_cast<const float4*>(V[v].Hit), reinterpret_cast<const float4*>(V[v].Surface), W, H, x, y);
+    }
+  }
+  retire(&S->counters[kResolveNext], &S->counters[kResolveDone], THREADS);
 }
 
 template <class K>
@@ -226,13 +257,15 @@ enum Parts { kTrace = 1, kShade = 2 };
 
 template <int T>
 int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratch* S, cudaStream_t s, int parts) {
-  static int traceGrid = 0, shadeGrid = 0;
+  static int traceGrid = 0, shadeGrid = 0, resolveGrid = 0;
   if (!traceGrid) {
     traceGrid = residentBlocks(traceViewsK<T>, T, traceSmem(T));
     shadeGrid = residentBlocks(shadeViewsK<T>, T);
+    resolveGrid = residentBlocks(resolveViewsK<T>, T);
   }
   if (parts & kTrace) traceViewsK<T><<<traceGrid, T, traceSmem(T), s>>>(V, n, t.grab, t.order, S);
   if (parts & kShade) shadeViewsK<T><<<shadeGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
+  if (parts & kShade) resolveViewsK<T><<<resolveGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
   return launchStatus();
 }
 

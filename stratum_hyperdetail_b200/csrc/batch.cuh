@@ -15,6 +15,8 @@ enum : int {
   kShadeNext = 2,
   kShadeDone = 3,
   kTotalTiles = 4,  // tiles over all views (written by the prologue)
+  kResolveNext = 5,
+  kResolveDone = 6,
   kCounters = 16
 };
 struct BatchScratch {

@@ -64,7 +64,7 @@ struct CoopRay {
   int cx, cz, sx, sz, ddaSteps;
   // current lot
   int slot, lcx, lcz;
-  f3 lr, ld, inv0, inv1;
+  f3 lr, ld, inv0;
   // hierarchy walk
   unsigned long long stack;
   int node, qsteps, pend, state;
@@ -124,7 +124,6 @@ SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __res
       r.lr = toLot(r.ro - cp, turn);
       r.ld = toLot(r.rd, turn);
       r.inv0 = invDir(r.ld);
-      r.inv1 = invDir(mk(r.ld.z, r.ld.y, -r.ld.x));
       // the DDA steps to the next cell now; the reference does it after the
       // lot's query, and the next test reads only t and the (later) best
       if (r.tx < r.tz) { r.t = r.tx; r.tx += r.dx; r.cx += r.sx; } else { r.t = r.tz; r.tz += r.dz; r.cz += r.sz; }
@@ -155,12 +154,19 @@ SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __res
   }
 }
 
+// Inverse of the turn-1 direction (ld.z, ld.y, -ld.x): a permutation of inv0
+// with one sign flipped, except for an exactly zero ld.x, whose guarded inverse
+// keeps the sign of the zero.
+SD f3 inv1Of(const CoopRay& r) {
+  return mk(r.inv0.z, r.inv0.y, r.ld.x == 0.0f ? guardedInv(-r.ld.x) : -r.inv0.x);
+}
+
 // One feature against a lane's ray in its lot frame, with the lot's
 // precomputed directions and inverses (turn 0 and turn 1 frames).
 SD float coopHit(const Feat& f, const CoopRay& r) {
   const bool odd = f.turn % 2 == 1;
   const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
-  return featureHitCore(f, r.lr, r.ld, intoFeature(r.lr - f.p, f.turn), d, odd ? r.inv1 : r.inv0, r.cone);
+  return featureHitCore(f, r.lr, r.ld, intoFeature(r.lr - f.p, f.turn), d, odd ? inv1Of(r) : r.inv0, r.cone);
 }
 
 // The winner's record for one lane: from the group cache when it holds the
@@ -279,7 +285,7 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
           for (int k = c * kRun; k < kEnd; k++) {
             const Feat f = unstage(ws.feats[myq][k]);
             const bool odd = f.turn % 2 == 1;
-            const f3 inv = odd ? r.inv1 : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
+            const f3 inv = odd ? inv1Of(r) : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
             const Span rg = featureSlab(f, p, inv);
             if (featureSlabMiss(f, rg)) continue;
             const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
