@@ -72,9 +72,10 @@ OPS_PER_RAY = {  # pose: (whole path, trace only)
     "park": (10787.8, 9618.4),
     "avenue": (20391.0, 19066.5),
 }
-# DRAM bytes per traced ray of tracePrimary from an ncu capture of the street
-# pose (profiles/tracePrimary_street_1600x900.md); None until captured.
-TRACE_DRAM_BYTES_PER_RAY = None
+# DRAM bytes per traced ray of traceViewsK: dram__bytes_read.sum +
+# dram__bytes_write.sum of one six-view 1600x900 launch (warm group cache, cold
+# L2 under ncu) = 110.6 MB + 237.7 MB over 8.64 M rays.
+TRACE_DRAM_BYTES_PER_RAY = 40.3
 
 METRIC = "shaded rays/s @1600x900"
 
@@ -663,7 +664,9 @@ def ours_arm(args):
     traffic = (TRACE_DRAM_BYTES_PER_RAY * rays_per_step) if TRACE_DRAM_BYTES_PER_RAY else None
     whole_ops = sum(OPS_PER_RAY[n][0] for n in names) * WIDTH * HEIGHT * args.steps
     roofline = {"bound": "fp32", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "kernel": "traceViewsK (one launch per step)",
+                "frac": achieved / peak, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one six-view launch, bytes",
+                "kernel": "traceViewsK (one launch per step)",
                 "peak_source": "measured in this run (stratum_issueProbe: FP32 lane ops/s, no FMA)",
                 "ops_source": "algorithmic FP32 ops per ray from the reference source (oracle/count_work.py)",
                 "path_frac": whole_ops / elapsed * world / world / peak,

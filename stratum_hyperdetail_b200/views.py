@@ -69,6 +69,15 @@ class View:
         self.C[19] = 0.0
         self.refresh(stream)
 
+    def save_ppm(self, path) -> None:
+        """Write the last resolved frame (Pixels, RGBA8) as a binary PPM (P6):
+        the reference harness's image format (tests/native_harness.cpp:115),
+        rows in buffer order, R, G, B from the low three bytes."""
+        px = self.Pixels.cpu().numpy().view(np.uint8).reshape(self.height, self.width, 4)[..., :3]
+        with open(path, "wb") as f:
+            f.write(f"P6\n{self.width} {self.height}\n255\n".encode())
+            f.write(np.ascontiguousarray(px).tobytes())
+
     def refresh(self, stream=None):
         s = _s(stream)
         call("stratum_clearQueue", ptr(self.Queue), s)
