@@ -68,6 +68,7 @@ struct CoopRay {
   // hierarchy walk
   unsigned long long stack;
   int node, qsteps, pend, state;
+  int fresh;  // node's entry was just found nearer than best (by its parent's test)
 };
 
 SD int popNode(unsigned long long& stack) {
@@ -81,7 +82,7 @@ SD void coopBegin(CoopRay& r, f3 ro, f3 rd, float cone, bool active) {
   r.ro = ro; r.rd = rd; r.cone = cone;
   r.best = kFar; r.fid = kSkyId; r.wslot = -1; r.wcx = r.wcz = 0;
   r.state = active ? kEnterLot : kDone;
-  r.stack = 0ull; r.node = 0; r.qsteps = 0; r.pend = 0; r.slot = 0; r.lcx = r.lcz = 0;
+  r.stack = 0ull; r.node = 0; r.qsteps = 0; r.pend = 0; r.slot = 0; r.lcx = r.lcz = 0; r.fresh = 0;
   r.ddaSteps = 0;
   if (!active) return;
   if (rd.y < -0.000001f) {
@@ -128,18 +129,23 @@ SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __res
       // lot's query, and the next test reads only t and the (later) best
       if (r.tx < r.tz) { r.t = r.tx; r.tx += r.dx; r.cx += r.sx; } else { r.t = r.tz; r.tz += r.dz; r.cz += r.sz; }
       if (nodeEntry(N, r.slot * kNodes + 1, r.lr, r.inv0, r.best) < r.best) {
-        r.state = kInLot; r.node = 1; r.stack = 0ull; r.qsteps = 0;
+        r.state = kInLot; r.node = 1; r.stack = 0ull; r.qsteps = 0; r.fresh = 1;
       }
       continue;
     }
     if (r.node <= 0 || r.qsteps >= kNodes) { r.state = kEnterLot; continue; }
     r.qsteps++;
     const int base = r.slot * kNodes;
-    float nearT = nodeEntry(N, base + r.node, r.lr, r.inv0, r.best);
-    if (nearT < r.best && r.node < kGroups) {
+    // A node reached from its parent was tested against the same best a
+    // moment ago (the reference tests it again, with the same result); a node
+    // popped from the stack is tested again against the current best.
+    const bool near = r.fresh || nodeEntry(N, base + r.node, r.lr, r.inv0, r.best) < r.best;
+    r.fresh = 0;
+    if (near && r.node < kGroups) {
       int left = r.node * 2, right = left + 1;
       float ln = nodeEntry(N, base + left, r.lr, r.inv0, r.best), rn = nodeEntry(N, base + right, r.lr, r.inv0, r.best);
       bool lh = ln < r.best, rh = rn < r.best;
+      r.fresh = lh || rh;
       if (lh && rh) {
         int next = ln < rn ? left : right, other = ln < rn ? right : left;
         r.stack = (r.stack << 7) | (unsigned long long)other;
@@ -148,7 +154,7 @@ SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __res
       else if (rh) r.node = right;
       else r.node = popNode(r.stack);
     } else {
-      if (nearT < r.best && r.node >= kGroups) { r.state = kLeafPending; r.pend = r.node - kGroups; break; }
+      if (near && r.node >= kGroups) { r.state = kLeafPending; r.pend = r.node - kGroups; break; }
       r.node = popNode(r.stack);
     }
   }
