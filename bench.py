@@ -113,13 +113,32 @@ def dist_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def init_dist(world):
+def init_dist(world, backend="nccl"):
+    """The process group of an N-rank run (None for one rank).  Ranks are
+    replicas: the only collectives are a barrier before the timed region and
+    the max-over-ranks reduction of its duration."""
     if world <= 1:
         return None
     import datetime
     import torch.distributed as dist
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist
+
+
+def max_over_ranks(dist, value, device="cuda"):
+    """The largest `value` over all ranks; every rank calls this (one all-reduce)."""
+    if not dist:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank, slowest_seconds, world):
+    """Whole-job throughput of `world` replicas that each processed
+    `units_per_rank` units, timed by the slowest rank."""
+    return units_per_rank * world / slowest_seconds
 
 
 # ---------------------------------------------------------------- clocks
@@ -644,18 +663,18 @@ def ours_arm(args):
         launches = batch.launches_per_frame * args.steps
         path = "batched: all views per launch, persistent tile queue, CUDA graph replay"
     else:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
         with ClockSampler(local) as clocks:
             wall0 = time.perf_counter()
             step_ms, _ = timed_steps(torch, stream, args.steps, flush, lambda: batch.frame(stream))
             wall = time.perf_counter() - wall0
         launches = batch.launches_per_frame * args.steps
         path = "batched: all views per launch, persistent tile queue (eager; graph capture failed)"
-    elapsed = sum(step_ms) * 1e-3
-    if dist:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-    value = rays_per_step * args.steps * world / elapsed
+    elapsed = max_over_ranks(dist, sum(step_ms) * 1e-3)
+    value = replica_throughput(rays_per_step * args.steps, elapsed, world)
 
     # -- roofline of the dominant kernel (traceViewsK): algorithmic FP32 ops / its event time
     peak = issue_peak(torch, sb)
