@@ -154,10 +154,10 @@ typedef struct stratum_view {
 /* Group cache of one table: the feature records of the (lot, group) pairs the
  * batched trace has evaluated, filled on first use and loaded afterwards
  * instead of being rebuilt by the grammar.  `entries` groups of at most 56
- * records (1,856 bytes each) plus a 4 MiB directory.  Entries are checked
+ * records (2,192 bytes each, with their culling boxes) plus a 4 MiB directory.  Entries are checked
  * against the table's current descriptor rows, so the cache never needs
  * invalidating when the table is refreshed (by any entry point); a full cache
- * is emptied at the start of the next batched frame.  A trace launch uses the
+ * keeps serving its groups and is emptied at most every 8 batched frames.  A trace launch uses the
  * groups filled by earlier launches (the first frame of a view fills, the
  * following ones reuse; at most 16,777,214 entries).  Results are identical
  * with and without a cache.  Initialise once before use (zeroes the directory,
@@ -269,7 +269,7 @@ typedef struct stratum_request_info {
 stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_views, int streams,
                                       const stratum_tune* tune);
 void stratum_server_destroy(stratum_server* server);
-/* Group cache entries of every session's table (default 65,536: 120 MiB per
+/* Group cache entries of every session's table (default 16,384: 38 MiB per
  * session, counted in the budget; 0: none).  Only before the first open. */
 int stratum_server_set_group_cache(stratum_server* server, int entries);
 /* Register a session (not yet resident: admission happens with its first request). */

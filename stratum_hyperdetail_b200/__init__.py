@@ -31,7 +31,7 @@ OK = 0
 EINVAL = -100000
 ELIMIT = -100001  # a fixed capacity of the library was exceeded
 NOALLOC_MAX_VIEWS = 64
-GROUP_CACHE_ENTRIES = 65536  # default group cache of a batched view: 116 MiB + 4 MiB directory
+GROUP_CACHE_ENTRIES = 65536  # default group cache of a batched view: 137 MiB + 4 MiB directory
 QUEUE_STALLED = 1
 BUDGET_EXCEEDED = 2
 NOT_FOUND = 3

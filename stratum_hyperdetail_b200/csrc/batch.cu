@@ -7,10 +7,12 @@
 //   clearViewsK,
 //   refreshViewsK   clearQueue + prepareLots of all views (grid: slots x views)
 //   buildViewsK     all views' queued lots, one 64-thread block per lot
-//   cacheResetK     empties the group caches that filled up (group_cache.cuh)
 //   prologueK       tile bases of every view under the chosen tile order, the
-//                   per-view frame constants (camera basis, sun, origin) and
-//                   the resolve taps, computed once per frame
+//                   per-view frame constants (camera basis, sun, origin), the
+//                   resolve taps and the group caches' launch epochs, computed
+//                   once per frame
+//   cacheResetK     clears the directory of a full group cache the prologue
+//                   chose to reset (group_cache.cuh)
 //   traceViewsK     persistent: each warp claims `grab` 8x4-pixel tiles at a
 //                   time from a device queue over all views and traces them
 //   shadeViewsK     persistent: shading of the same tiles (Linear)
@@ -70,20 +72,19 @@ __global__ void __launch_bounds__(64) buildViewsK(const stratum_view* __restrict
   buildQueue(V[v].Queue, V[v].World, V[v].Nodes, int(blockIdx.x), int(gridDim.x), sm);
 }
 
-// A full group cache is emptied at the start of a frame: its directory is
-// zeroed here, its fill counter reset by the prologue that follows.
+// The directory of a group cache whose reset the prologue just decided.
 __global__ void cacheResetK(const stratum_view* __restrict__ V, int n) {
   const int v = int(blockIdx.y);
   if (v >= n || !V[v].Groups) return;
   const GroupCacheHeader* h = reinterpret_cast<const GroupCacheHeader*>(V[v].Groups);
-  if (h->capacity == 0u || h->next < h->capacity) return;
+  if (h->capacity == 0u || h->resetAt != h->launches || h->resets == 0u) return;
   uint4* d = reinterpret_cast<uint4*>(groupCache(V[v].Groups).dir(0, 0));
   for (int i = int(blockIdx.x * blockDim.x + threadIdx.x); i < kCacheDirWords / 4; i += int(gridDim.x * blockDim.x))
     d[i] = make_uint4(0u, 0u, 0u, 0u);
 }
 __global__ void cacheInitK(uint32_t* base, uint32_t entries) {
   GroupCacheHeader* h = reinterpret_cast<GroupCacheHeader*>(base);
-  h->next = 0u; h->capacity = entries; h->resets = 0u; h->fills = 0u; h->launches = 0u;
+  h->next = 0u; h->capacity = entries; h->resets = 0u; h->fills = 0u; h->launches = 0u; h->resetAt = 0u;
 }
 
 __global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
@@ -100,10 +101,14 @@ __global__ void prologueK(stratum_view* V, int n, int order, BatchScratch* S) {
   }
   for (int v = int(threadIdx.x); v < n; v += int(blockDim.x)) {
     S->view[v] = makeFrame(V[v].C, V[v].Origin);
-    if (V[v].Groups) {  // after cacheResetK: a full cache starts again
+    if (V[v].Groups) {  // this launch's epoch; a full cache starts again now and then
       GroupCacheHeader* h = reinterpret_cast<GroupCacheHeader*>(V[v].Groups);
-      if (h->capacity != 0u && h->next >= h->capacity) { h->next = 0u; h->resets++; }
-      h->launches++;  // this launch's epoch
+      h->launches++;
+      if (h->capacity != 0u && h->next >= h->capacity && h->launches - h->resetAt >= kCacheResetInterval) {
+        h->next = 0u;
+        h->resets++;
+        h->resetAt = h->launches;  // cacheResetK clears the directory next
+      }
     }
   }
 }
@@ -282,8 +287,8 @@ int render(stratum_view* V, int n, void* scratch, unsigned long long bytes, cons
   if (!tuneOk(t)) return STRATUM_EINVAL;
   BatchScratch* S = static_cast<BatchScratch*>(scratch);
   if (parts & kTrace) {
-    cacheResetK<<<dim3(64, n), 256, 0, s>>>(V, n);
     prologueK<<<1, 256, 0, s>>>(V, n, t.order, S);
+    cacheResetK<<<dim3(64, n), 256, 0, s>>>(V, n);
   }
   if (t.threads == 64) return launchParts<64>(V, n, t, S, s, parts);
   if (t.threads == 256) return launchParts<256>(V, n, t, S, s, parts);

@@ -9,8 +9,9 @@
 //                    trace launches
 //   dir      16,384 x 64 u32: per (slot, group) 0 = empty, kCacheBusy = being
 //            filled, else (launch epoch << 24) | (entry index + 1)
-//   entries  capacity x 1,856 B: a 64-byte tag (the lot descriptor words the
-//            grammar reads, the group, the count) and 56 records of 32 bytes
+//   entries  capacity x 2,192 B: a 64-byte tag (the lot descriptor words the
+//            grammar reads, the group, the count), 56 records of 32 bytes and
+//            the 14 chunk boxes of runs of 4 records (24 bytes each)
 //
 // An entry serves a (slot, group) only while its tag equals the slot's current
 // descriptor words and the group, so a table refreshed by any path (batched or
@@ -22,8 +23,10 @@
 // warp that misses claims the group (one atomic compare-and-swap on its
 // directory word) and fills an entry, or, when another warp holds it or the
 // store is full, builds the records with the grammar itself: nothing waits.
-// When the store is full at the start of a launch, the directory is cleared
-// and filling starts again.
+// A full store keeps serving the groups it holds; at the start of a launch at
+// least kCacheResetInterval launches after its last reset, a full store is
+// emptied (directory cleared) and filling starts again, so tables that change
+// or need more groups than fit are re-cached from time to time.
 #pragma once
 #include "grammar_ra.cuh"
 
@@ -46,16 +49,19 @@ SD Feat unstage(const StagedFeat& s) {
 }
 
 struct GroupCacheHeader {
-  uint32_t next, capacity, resets, fills, launches;
-  uint32_t pad[59];
+  uint32_t next, capacity, resets, fills, launches, resetAt;  // resetAt: launch count of the last reset
+  uint32_t pad[58];
 };
 static_assert(sizeof(GroupCacheHeader) == 256, "group cache header is 256 bytes");
 constexpr uint32_t kCacheBusy = 0xFFFFFFFFu;
+constexpr uint32_t kCacheResetInterval = 8;  // launches between resets of a full store
 constexpr uint32_t kCacheMaxEntries = (1u << 24) - 2u;  // entry index + 1 fits 24 bits and is never 0xFFFFFF
 constexpr int kCacheDirWords = kLots * kGroups;
 constexpr int kEntryRecords = 56;  // the largest group (group 30 of a building lot)
 constexpr int kEntryTagWords = 16;  // 64 bytes, 11 used
-constexpr size_t kEntryBytes = size_t(kEntryTagWords) * 4 + size_t(kEntryRecords) * sizeof(StagedFeat);
+constexpr int kEntryBoxes = 14;     // chunk boxes of runs of 4 records, as the trace stages them
+constexpr size_t kEntryBoxOffset = size_t(kEntryTagWords) * 4 + size_t(kEntryRecords) * sizeof(StagedFeat);
+constexpr size_t kEntryBytes = kEntryBoxOffset + size_t(kEntryBoxes) * 24;
 constexpr size_t kCacheDirOffset = sizeof(GroupCacheHeader);
 constexpr size_t kCacheEntryOffset = kCacheDirOffset + size_t(kCacheDirWords) * 4;
 static_assert(kEntryBytes % 16 == 0 && kCacheEntryOffset % 16 == 0, "entries are 16-byte aligned");
@@ -81,6 +87,7 @@ SD uint32_t* entryTag(const GroupCache& c, uint32_t e) { return reinterpret_cast
 SD StagedFeat* entryRecords(const GroupCache& c, uint32_t e) {
   return reinterpret_cast<StagedFeat*>(c.entry(e) + kEntryTagWords * 4);
 }
+SD float* entryBoxes(const GroupCache& c, uint32_t e) { return reinterpret_cast<float*>(c.entry(e) + kEntryBoxOffset); }
 
 // The entry a directory word names if it was filled by an earlier launch, else -1.
 SD int usableEntry(const GroupCache& c, uint32_t d) {
@@ -122,7 +129,7 @@ SD int cacheClaim(const GroupCache& c, int slot, int group, uint32_t old) {
   int e = -1;
   if ((threadIdx.x & 31) == 0) {
     uint32_t* dp = c.dir(slot, group);
-    if (atomicCAS(dp, old, kCacheBusy) == old) {
+    if (__ldcg(&c.hdr()->next) < c.capacity() && atomicCAS(dp, old, kCacheBusy) == old) {
       const uint32_t i = atomicAdd(&c.hdr()->next, 1u);
       if (i < c.capacity()) e = int(i);
       else atomicExch(dp, old);  // full: leave the word as it was

@@ -10,10 +10,12 @@
 // Admission is by an HBM budget: a session is admitted when its bytes fit;
 // otherwise least recently used sessions that are idle (nothing queued in a
 // launched batch) are evicted.  Eviction snapshots what the future needs (camera
-// state, table origin, accumulation buffer) to host memory and frees the
+// state, table origin, accumulation buffer) to pinned host memory and frees the
 // device memory; re-admission restores the snapshot and rebuilds the table and
 // hierarchy from the seed, so the session continues exactly as if it had never
-// left (the world is a pure function of seed and address).
+// left (the world is a pure function of seed and address).  Eviction and
+// admission are ordered on one admission stream that batches wait for with an
+// event: the scheduler thread never waits on the device for them.
 //
 // The scheduler thread keeps `streams` batch slots.  Whenever a slot is free it
 // takes the oldest pending request of every idle session (up to `max_views`),
@@ -86,9 +88,9 @@ struct Session {
   stratum_pose last{};
   double lastUse = 0.0;
   bool hasSnap = false;
-  std::vector<float> snapC;
-  float* snapHist = nullptr;  // pinned: the accumulation buffer while evicted (kept for the next eviction)
-  unsigned snapOrigin[4] = {0, 0, 0, 0};
+  // pinned snapshot while evicted (kept for the next eviction): History (P x 16 B),
+  // then C (256 B) and Origin (16 B)
+  char* snap = nullptr;
   unsigned char* pinnedOut = nullptr;
   template <class T> T* at(size_t off) const { return reinterpret_cast<T*>(base + off); }
   stratum_view view() const {
@@ -126,13 +128,14 @@ struct stratum_server {
   int device = 0;
   unsigned long long budget = 0;
   int maxViews = 1;
-  int groupEntries = 65536;
+  int groupEntries = 16384;
   stratum_tune tune{64, 1, 1};
   std::mutex mu;
   std::condition_variable cv;
   std::thread worker;
   std::atomic<bool> stop{false};
   cudaStream_t admitStream = nullptr;
+  cudaEvent_t admitDone = nullptr;  // recorded after each admission's device work
   std::unordered_map<int, std::unique_ptr<Session>> sessions;
   int nextSession = 1;
   std::unordered_map<long long, std::unique_ptr<Request>> requests;
@@ -159,20 +162,21 @@ void finish(stratum_server* S, Request* r, int status) {
   }
 }
 
-// Snapshot what a session needs to continue, then free its device memory.
+// Snapshot what a session needs to continue, then free its device memory.  All
+// of it is ordered on the admission stream (copies, then the free; a later
+// re-admission's restore follows on the same stream), so nothing waits here.
+// Only idle sessions are evicted: their last batch has completed.
 int evict(stratum_server* S, Session& s) {
   size_t P = size_t(s.width) * size_t(s.height);
-  s.snapC.resize(64);
-  if (!s.snapHist && cudaMallocHost(reinterpret_cast<void**>(&s.snapHist), P * 16) != cudaSuccess) {
-    s.snapHist = nullptr;
+  if (!s.snap && cudaMallocHost(reinterpret_cast<void**>(&s.snap), P * 16 + 512) != cudaSuccess) {
+    s.snap = nullptr;
     return -int(cudaGetLastError());
   }
-  cudaError_t e = cudaMemcpyAsync(s.snapC.data(), s.at<float>(s.lay.C), 64 * 4, cudaMemcpyDeviceToHost, S->admitStream);
+  cudaError_t e = cudaMemcpyAsync(s.snap + P * 16, s.at<float>(s.lay.C), 64 * 4, cudaMemcpyDeviceToHost, S->admitStream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.snapOrigin, s.at<unsigned>(s.lay.Origin), 16, cudaMemcpyDeviceToHost, S->admitStream);
+    e = cudaMemcpyAsync(s.snap + P * 16 + 256, s.at<unsigned>(s.lay.Origin), 16, cudaMemcpyDeviceToHost, S->admitStream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s.snapHist, s.at<float>(s.lay.History), P * 16, cudaMemcpyDeviceToHost, S->admitStream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(S->admitStream);
+    e = cudaMemcpyAsync(s.snap, s.at<float>(s.lay.History), P * 16, cudaMemcpyDeviceToHost, S->admitStream);
   if (e != cudaSuccess) return -int(e);
   cudaFreeAsync(s.base, S->admitStream);
   s.base = nullptr;
@@ -217,19 +221,19 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
                                 reinterpret_cast<stratum_stream_t>(S->admitStream));
   if (st == STRATUM_OK && s.hasSnap) {  // continue exactly where the session left
     size_t P = size_t(s.width) * size_t(s.height);
-    e = cudaMemcpyAsync(s.at<float>(s.lay.C), s.snapC.data(), 64 * 4, cudaMemcpyHostToDevice, S->admitStream);
+    e = cudaMemcpyAsync(s.at<float>(s.lay.C), s.snap + P * 16, 64 * 4, cudaMemcpyHostToDevice, S->admitStream);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s.at<unsigned>(s.lay.Origin), s.snapOrigin, 16, cudaMemcpyHostToDevice, S->admitStream);
+      e = cudaMemcpyAsync(s.at<unsigned>(s.lay.Origin), s.snap + P * 16 + 256, 16, cudaMemcpyHostToDevice, S->admitStream);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(s.at<float>(s.lay.History), s.snapHist, P * 16, cudaMemcpyHostToDevice, S->admitStream);
+      e = cudaMemcpyAsync(s.at<float>(s.lay.History), s.snap, P * 16, cudaMemcpyHostToDevice, S->admitStream);
     if (e != cudaSuccess) st = -int(e);
   }
   if (st == STRATUM_OK && !s.pinnedOut) {
     e = cudaMallocHost(reinterpret_cast<void**>(&s.pinnedOut), size_t(s.width) * s.height * 4);
     if (e != cudaSuccess) st = -int(e);
   }
-  if (st == STRATUM_OK) {
-    e = cudaStreamSynchronize(S->admitStream);
+  if (st == STRATUM_OK) {  // batches wait for this event on their own streams; the host does not
+    e = cudaEventRecord(S->admitDone, S->admitStream);
     if (e != cudaSuccess) st = -int(e);
   }
   if (st != STRATUM_OK) {
@@ -265,7 +269,10 @@ int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
   }
   cudaStream_t st = sl.stream;
   stratum_stream_t ss = reinterpret_cast<stratum_stream_t>(st);
-  cudaError_t e = cudaMemcpyAsync(sl.dViews, sl.hViews, sizeof(stratum_view) * n, cudaMemcpyHostToDevice, st);
+  // sessions admitted for this batch: their allocation, initialisation and
+  // restored snapshot are ordered on the admission stream
+  cudaError_t e = cudaStreamWaitEvent(st, S->admitDone, 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sl.dViews, sl.hViews, sizeof(stratum_view) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.dPoses, sl.hPoses, sizeof(stratum_pose) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.dFlags, sl.hFlags, sizeof(int) * n, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return -int(e);
@@ -371,8 +378,8 @@ void freeSession(stratum_server* S, Session& s) {
   }
   if (s.pinnedOut) cudaFreeHost(s.pinnedOut);
   s.pinnedOut = nullptr;
-  if (s.snapHist) cudaFreeHost(s.snapHist);
-  s.snapHist = nullptr;
+  if (s.snap) cudaFreeHost(s.snap);
+  s.snap = nullptr;
 }
 
 }  // namespace
@@ -387,7 +394,9 @@ stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_v
   S->budget = budget_bytes;
   S->maxViews = max_views;
   if (tune) S->tune = *tune;
-  if (cudaStreamCreateWithFlags(&S->admitStream, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+  if (cudaStreamCreateWithFlags(&S->admitStream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&S->admitDone, cudaEventDisableTiming) != cudaSuccess)
+    return nullptr;
   S->slots.resize(streams);
   for (Slot& sl : S->slots) {
     sl.scratchBytes = stratum_batchScratchBytes(max_views);
@@ -435,6 +444,7 @@ void stratum_server_destroy(stratum_server* S) {
     if (sl.done) cudaEventDestroy(sl.done);
     if (sl.stream) cudaStreamDestroy(sl.stream);
   }
+  if (S->admitDone) cudaEventDestroy(S->admitDone);
   if (S->admitStream) cudaStreamDestroy(S->admitStream);
   delete S;
 }

@@ -32,22 +32,36 @@ namespace st {
 static __device__ __noinline__ Feat featureAtOOL(LotDesc L, int g, int i) { return featureAt(L, g, i); }
 
 // Sub-group culling: every run of kRun staged features gets a box (in the
-// lot frame) that contains every point where any of them can be hit, and a
-// lane tests a run's features only when its ray enters that box nearer than
-// its current best.  Hits lie inside a feature's bounds box (shapes 0-4, 7)
-// or within the 0.025 m masonry pad of it; leaf discs of foliage envelopes can
-// reach one 0.18 m grid cell (0.31 m diagonal) beyond the envelope's box, so
-// foliage gets a 0.35 m pad.  A skipped feature could only have been rejected,
-// so results are unchanged.
+// lot frame) that contains every distance any of them can return, and a lane
+// tests a run's features only when its ray enters that box nearer than its
+// current best, so a skipped feature could only have been rejected and
+// results are unchanged.  That holds for the features whose computed distance
+// is a slab entry of their own box or follows from it: plain boxes and prisms
+// (the slab entry, or a roof plane behind it), masonry boxes (relief moves the
+// hit at most 0.0025 m toward the ray per unit of the face normal, inside the
+// 0.025 m pad) and foliage envelopes (leaf discs reach at most one 0.18 m grid
+// cell, 0.31 m diagonal, beyond the envelope's box: 0.35 m pad).  Ellipsoids,
+// cylinders and arches/rings solve a quadratic whose float result can land
+// well outside the box at long range (cancellation; 0.17 m at 1.4 km was
+// seen), so a run holding one of them gets an unbounded box and is never
+// skipped.  (Testing those alone in a culled run, or staging them apart,
+// measured slower: lanes then diverge inside the run.)
 #ifndef STRATUM_COOP_RUN
 #define STRATUM_COOP_RUN 4
 #endif
 constexpr int kRun = STRATUM_COOP_RUN;
+static_assert(kRun * kEntryBoxes >= kEntryRecords, "a group cache entry holds every chunk box of a group");
 struct ChunkBox { float lo[3], hi[3]; };
 SD void hitBox(const Feat& f, f3& lo, f3& hi) {
+  const bool foliage = f.shape == 1 && f.material == 7;
+  if ((f.shape == 1 && !foliage) || f.shape == 2 || f.shape == 4 || f.shape == 7) {
+    lo = mk(-1e30f, -1e30f, -1e30f);  // quadric: its run is never skipped
+    hi = mk(1e30f, 1e30f, 1e30f);
+    return;
+  }
   f3 ext = f.h;
   if (f.turn % 2 == 1) ext = mk(f.h.z, f.h.y, f.h.x);
-  const float pad = (f.shape == 1 && f.material == 7) ? 0.35f : 0.025f;
+  const float pad = foliage ? 0.35f : 0.025f;
   lo = f.p - ext - mk(pad, pad, pad);
   hi = f.p + ext + mk(pad, pad, pad);
 }
@@ -219,29 +233,43 @@ SD int stageGroup(const float* __restrict__ W, const GroupCache& cache, int key,
   int e = cacheFind(cache, W, slot, g, count, word);
   const bool cached = e >= 0;
   if (!cached) e = cacheClaim(cache, slot, g, word);  // -1: build without storing
+  if (cached) {  // records and chunk boxes as stored
+    if (lane < count) ws.feats[q][lane] = cacheRecord(cache, e, lane);
+    if (lane + 32 < count) ws.feats[q][lane + 32] = cacheRecord(cache, e, lane + 32);
+    const int runs = (count + kRun - 1) / kRun;
+    if (lane < runs) {
+      const float2* bp = reinterpret_cast<const float2*>(entryBoxes(cache, uint32_t(e)) + lane * 6);
+      const float2 a = __ldg(bp), b = __ldg(bp + 1), c = __ldg(bp + 2);
+      ws.boxes[q][lane] = ChunkBox{{a.x, a.y, b.x}, {b.y, c.x, c.y}};
+    }
+  } else {
 #pragma unroll 1
-  for (int base = 0; base < count; base += 32) {
-    const int j = base + lane;
-    f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
-    if (j < count) {
-      StagedFeat s;
-      if (cached) {
-        s = cacheRecord(cache, e, j);
-      } else {
+    for (int base = 0; base < count; base += 32) {
+      const int j = base + lane;
+      f3 lo = mk(1e30f, 1e30f, 1e30f), hi = mk(-1e30f, -1e30f, -1e30f);
+      if (j < count) {
+        StagedFeat s;
         stage(s, featureAtOOL(L, g, j));
         if (e >= 0) entryRecords(cache, uint32_t(e))[j] = s;
+        ws.feats[q][j] = s;
+        hitBox(unstage(s), lo, hi);
       }
-      ws.feats[q][j] = s;
-      hitBox(unstage(s), lo, hi);
-    }
 #pragma unroll
-    for (int o = 1; o < kRun; o <<= 1) {
-      lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
-                       __shfl_xor_sync(0xffffffffu, lo.z, o)));
-      hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
-                       __shfl_xor_sync(0xffffffffu, hi.z, o)));
+      for (int o = 1; o < kRun; o <<= 1) {
+        lo = vmin(lo, mk(__shfl_xor_sync(0xffffffffu, lo.x, o), __shfl_xor_sync(0xffffffffu, lo.y, o),
+                         __shfl_xor_sync(0xffffffffu, lo.z, o)));
+        hi = vmax(hi, mk(__shfl_xor_sync(0xffffffffu, hi.x, o), __shfl_xor_sync(0xffffffffu, hi.y, o),
+                         __shfl_xor_sync(0xffffffffu, hi.z, o)));
+      }
+      if ((lane & (kRun - 1)) == 0 && j < count) {
+        const ChunkBox b = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
+        ws.boxes[q][j / kRun] = b;
+        if (e >= 0) {
+          float* bp = entryBoxes(cache, uint32_t(e)) + (j / kRun) * 6;
+          bp[0] = b.lo[0]; bp[1] = b.lo[1]; bp[2] = b.lo[2]; bp[3] = b.hi[0]; bp[4] = b.hi[1]; bp[5] = b.hi[2];
+        }
+      }
     }
-    if ((lane & (kRun - 1)) == 0 && j < count) ws.boxes[q][j / kRun] = ChunkBox{{lo.x, lo.y, lo.z}, {hi.x, hi.y, hi.z}};
   }
   if (!cached && e >= 0) cachePublish(cache, W, slot, g, count, e);
   return count;

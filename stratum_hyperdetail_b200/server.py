@@ -76,7 +76,7 @@ class Server:
     def __init__(self, budget_bytes: int, max_views: int = 16, streams: int = 3, tune=(64, 1, 1),
                  group_cache: int | None = None):
         """`group_cache`: group cache entries per session (None: the library's
-        default of 65,536; 0: none)."""
+        default of 16,384; 0: none)."""
         self.L = _lib()
         t = Tune(*tune)
         self.h = self.L.stratum_server_create(int(budget_bytes), int(max_views), int(streams), ct.byref(t))
