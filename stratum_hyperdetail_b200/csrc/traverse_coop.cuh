@@ -43,9 +43,13 @@ static __device__ __noinline__ Feat featureAtOOL(LotDesc L, int g, int i) { retu
 // cell, 0.31 m diagonal, beyond the envelope's box: 0.35 m pad).  Ellipsoids,
 // cylinders and arches/rings solve a quadratic whose float result can land
 // well outside the box at long range (cancellation; 0.17 m at 1.4 km was
-// seen), so a run holding one of them gets an unbounded box and is never
-// skipped.  (Testing those alone in a culled run, or staging them apart,
-// measured slower: lanes then diverge inside the run.)
+// seen), so their box is only bounded along the axis the intersection code
+// itself checks: a cylinder's side hit is kept only when its height is within
+// +-h.y and its caps lie at +-h.y, so its distance is inside the y slab; an
+// arch or ring keeps hits within +-h.z of its own frame (lot x or z by its
+// turn); an ellipsoid's root is not checked at all, so its box is unbounded.
+// (Testing quadrics alone in a culled run, or staging them apart, measured
+// slower: lanes then diverge inside the run.)
 #ifndef STRATUM_COOP_RUN
 #define STRATUM_COOP_RUN 4
 #endif
@@ -54,16 +58,23 @@ static_assert(kRun * kEntryBoxes >= kEntryRecords, "a group cache entry holds ev
 struct ChunkBox { float lo[3], hi[3]; };
 SD void hitBox(const Feat& f, f3& lo, f3& hi) {
   const bool foliage = f.shape == 1 && f.material == 7;
-  if ((f.shape == 1 && !foliage) || f.shape == 2 || f.shape == 4 || f.shape == 7) {
-    lo = mk(-1e30f, -1e30f, -1e30f);  // quadric: its run is never skipped
-    hi = mk(1e30f, 1e30f, 1e30f);
-    return;
-  }
   f3 ext = f.h;
   if (f.turn % 2 == 1) ext = mk(f.h.z, f.h.y, f.h.x);
   const float pad = foliage ? 0.35f : 0.025f;
   lo = f.p - ext - mk(pad, pad, pad);
   hi = f.p + ext + mk(pad, pad, pad);
+  const float open = 1e30f;
+  if (f.shape == 1 && !foliage) {  // ellipsoid: unbounded
+    lo = mk(-open, -open, -open);
+    hi = mk(open, open, open);
+  } else if (f.shape == 2) {  // cylinder: the y slab only
+    lo.x = lo.z = -open;
+    hi.x = hi.z = open;
+  } else if (f.shape == 4 || f.shape == 7) {  // arch, ring: its own z slab only (lot x when the turn is odd)
+    lo.y = -open;
+    hi.y = open;
+    if (f.turn % 2 == 1) { lo.z = -open; hi.z = open; } else { lo.x = -open; hi.x = open; }
+  }
 }
 
 enum LaneState : int { kEnterLot = 0, kInLot = 1, kLeafPending = 2, kDone = 3 };
