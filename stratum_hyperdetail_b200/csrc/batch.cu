@@ -138,13 +138,14 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
   }
 }
 
-// STRATUM_TRACE_OCC / THREADS resident blocks.  768 threads per SM (24 warps,
-// 80 registers per thread with a few spills) measured faster than 512 (128
-// registers, no spills): the traversal is latency-bound.
+// STRATUM_TRACE_OCC / THREADS resident blocks (rounded down).  640 threads per
+// SM (96 registers per thread for 64- and 128-thread blocks, 128 for 256) and
+// 576 or 704 measured alike, 6-8 % faster than 768 (80 registers, heavy
+// spills) with the group cache in place.
 // The warp-cooperative traversal (traverse_coop.cuh) unless built with
 // STRATUM_BATCH_PER_LANE (each lane walks its own ray, as the drop-in kernel).
 #ifndef STRATUM_TRACE_OCC
-#define STRATUM_TRACE_OCC 768
+#define STRATUM_TRACE_OCC 640
 #endif
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
