@@ -219,8 +219,13 @@ __global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) shadeVie
   retire(&S->counters[kShadeNext], &S->counters[kShadeDone], THREADS);
 }
 
+// STRATUM_RESOLVE_OCC / THREADS resident blocks (0: the compiler's choice;
+// 1024, 1536 and 2048 threads per SM measured the same).
+#ifndef STRATUM_RESOLVE_OCC
+#define STRATUM_RESOLVE_OCC 0
+#endif
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) resolveViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
+__global__ void __launch_bounds__(THREADS, STRATUM_RESOLVE_OCC / THREADS) resolveViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
                                                         BatchScratch* S) {
   const int lane = int(threadIdx.x & 31);
   const int total = int(S->counters[kTotalTiles]);
