@@ -80,6 +80,13 @@ TRACE_DRAM_BYTES_PER_RAY = 41.6
 METRIC = "shaded rays/s @1600x900"
 
 
+def workload_config(names):
+    """The workload both arms report on (the six-pose 1600x900 frame)."""
+    return {"workload": "plain single-view frame 1600x900, seed 0x5EED, six poses, one sample per view per step "
+                        "accumulating toward 64",
+            "width": WIDTH, "height": HEIGHT, "views_per_step": len(names), "poses": {n: POSES[n] for n in names}}
+
+
 def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -444,8 +451,8 @@ def reference_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / len(times) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural world, fixed poses)",
-            "config": {"workload": "plain single-view frame 1600x900, seed 0x5EED, six poses", "width": WIDTH,
-                       "height": HEIGHT, "poses": list(POSES), "device": "host CPU"},
+            "config": {**workload_config(list(POSES)), "device": "host CPU",
+                       "path": "the reference renderer built from its own sources (oracle/_ref), all host threads"},
             "cpu_baseline": {"value": value, "unit": "rays/s", "cores": nthreads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -690,6 +697,16 @@ def ours_arm(args):
                 "ops_source": "algorithmic FP32 ops per ray from the reference source (oracle/count_work.py)",
                 "path_frac": whole_ops / elapsed * world / world / peak,
                 "plain_trace_frac": trace_ops / (trace_plain.sum() * 1e-3) / peak}
+    # the memory roofline of the same kernel, for contrast: its DRAM traffic per launch over the launch time
+    # against the pool's measured HBM copy bandwidth
+    hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    if peaks_file.exists():
+        hbm_peak, hbm_src = float(json.loads(peaks_file.read_text())["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    if traffic:
+        hbm_achieved = traffic / (trace_batch_ms * 1e-3 / args.steps) / 1e9
+        roofline["hbm"] = {"bound": "hbm", "achieved": hbm_achieved, "peak": hbm_peak, "unit": "GB/s",
+                           "frac": hbm_achieved / hbm_peak, "peak_source": hbm_src}
 
     # -- e2e: the batched C-ABI call with the step's inputs from pinned host memory and RGBA8 back
     host_in = [torch.zeros(32, dtype=torch.float32).pin_memory() for _ in views]
@@ -747,10 +764,7 @@ def ours_arm(args):
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded procedural world, fixed poses)",
-            "config": {"workload": "plain single-view frame 1600x900, seed 0x5EED, six poses, one sample per view "
-                                   "per step accumulating toward 64",
-                       "width": WIDTH, "height": HEIGHT, "views_per_step": n_views,
-                       "poses": {n: POSES[n] for n in names}, "path": path, "tune": tune,
+            "config": {**workload_config(names), "path": path, "tune": tune,
                        "l2": "flushed between timed steps (256 MiB write outside the timed region)",
                        "parallelism": f"replicas x{world}"},
             "plain_path": {"value": plain_value, "unit": "rays/s", "ms_per_step": sum(plain_ms) / args.steps,
