@@ -75,3 +75,17 @@ def test_engine_fails_loudly_without_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError):
         sb.Engine().init(320, 180)
+
+
+def test_group_cache_sizes():
+    """Group cache buffer = 256 B header + 16,384 x 64 directory words + entries
+    of 2,192 B (64 B tag, 56 records of 32 B, 14 run boxes of 24 B)."""
+    import stratum_hyperdetail_b200 as sb
+    L = sb.lib()
+    base = 256 + 16384 * 64 * 4
+    assert L.stratum_groupCacheBytes(0) == base
+    assert L.stratum_groupCacheBytes(1) == base + 2192
+    assert L.stratum_groupCacheBytes(sb.GROUP_CACHE_ENTRIES) == base + 2192 * sb.GROUP_CACHE_ENTRIES
+    assert L.stratum_groupCacheBytes(-1) == 0
+    assert L.stratum_groupCacheInit(None, 16, None) == sb.EINVAL
+    assert L.stratum_groupCacheInit(ct.c_void_p(256), 1 << 24, None) == sb.EINVAL  # above the 24-bit entry index
