@@ -189,3 +189,29 @@ def test_random_views_equal_plain(cuda):
         for i, (p, q) in enumerate(zip(plain, batched)):
             for k in ("Hit", "Surface", "Linear", "History", "Pixels"):
                 assert torch.equal(getattr(p, k), getattr(q, k)), f"frame {f} view {i}: {k} differs"
+
+
+def test_tiny_and_ragged_views_equal_plain(cuda):
+    """Views smaller than one 8x4 tile or with ragged edges (1x1, 7x3, 8x4,
+    9x5, 33x17) mixed in one batch: every pixel equals the single-view path."""
+    from stratum_hyperdetail_b200.batch import Batch
+    from stratum_hyperdetail_b200.views import View
+    sizes = [(1, 1), (7, 3), (8, 4), (9, 5), (33, 17)]
+
+    def views():
+        out = []
+        for i, (w, h) in enumerate(sizes):
+            v = View(w, h)
+            v.set_pose(100 + i, [i, 0, 2 * i, 0], (3.0 * i, 1.7 + 10 * i, -2.0), 0.4 * i, -0.1 * i)
+            out.append(v)
+        return out
+    plain, batched = views(), views()
+    b = Batch(batched, (64, 2, 1))
+    for f in range(3):
+        for v in plain:
+            v.frame(0.0)
+        b.frame()
+        torch.cuda.synchronize()
+        for i, (p, q) in enumerate(zip(plain, batched)):
+            for k in ("Hit", "Surface", "Linear", "History", "Pixels"):
+                assert torch.equal(getattr(p, k), getattr(q, k)), f"frame {f} view {sizes[i]}: {k} differs"
