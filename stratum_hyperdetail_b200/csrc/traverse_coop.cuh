@@ -192,14 +192,6 @@ SD f3 inv1Of(const CoopRay& r) {
   return mk(r.inv0.z, r.inv0.y, r.ld.x == 0.0f ? guardedInv(-r.ld.x) : -r.inv0.x);
 }
 
-// One feature against a lane's ray in its lot frame, with the lot's
-// precomputed directions and inverses (turn 0 and turn 1 frames).
-SD float coopHit(const Feat& f, const CoopRay& r) {
-  const bool odd = f.turn % 2 == 1;
-  const f3 d = odd ? mk(r.ld.z, r.ld.y, -r.ld.x) : r.ld;
-  return featureHitCore(f, r.lr, r.ld, intoFeature(r.lr - f.p, f.turn), d, odd ? inv1Of(r) : r.inv0, r.cone);
-}
-
 // The winner's record for one lane: from the group cache when it holds the
 // group, else from the grammar.
 SD Feat winnerFeature(const GroupCache& c, const float* __restrict__ W, int slot, int g, int i) {
