@@ -91,8 +91,8 @@ class Batch:
 
     @property
     def launches_per_frame(self) -> int:
-        # stepViews, clearViews, refreshViews, buildViews, cacheReset, prologue, trace, shade, resolve
-        return 9
+        # stepViews, clearViews, refreshViews, buildViews, prologue, cacheReset, trace, shade, light, resolve
+        return 10
 
     def capture(self):
         """Capture one batched frame as a CUDA graph (after one eager frame so

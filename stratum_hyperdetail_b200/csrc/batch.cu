@@ -15,7 +15,12 @@
 //                   chose to reset (group_cache.cuh)
 //   traceViewsK     persistent: each warp claims `grab` 8x4-pixel tiles at a
 //                   time from a device queue over all views and traces them
-//   shadeViewsK     persistent: shading of the same tiles (Linear)
+//   shadeViewsK     persistent: material colour of the same tiles (albedo into
+//                   Linear; sky pixels get their final colour)
+//   lightViewsK     persistent: lighting of the hit pixels from that albedo
+//                   (relief normal, sun shadow, ambient, GGX, reflections, fog)
+//                   into Linear -- two kernels because the shading code split in
+//                   two measured faster than one (instruction fetch)
 //   resolveViewsK   persistent: contact occlusion, accumulation and tone map
 //                   (History, Pixels); a kernel of its own because the two
 //                   fused measured slower (the shading code alone fills the
@@ -212,7 +217,16 @@ __global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) shadeVie
       const size_t b = size_t(y) * W + x;
       const float4* hit = reinterpret_cast<const float4*>(V[v].Hit);
       const float4* surf = reinterpret_cast<const float4*>(V[v].Surface);
-      f3 c = shadePixel(V[v].World, F, hit[b], surf[b], primaryDir(F.cam, x, y, W, H), H);
+      const float4 h4 = hit[b];
+      const f3 rd = primaryDir(F.cam, x, y, W, H);
+      f3 c;
+      if (int(h4.y) == kSkyId) {
+        c = skyColor(rd, F.sun);
+      } else {
+        SurfacePoint sp;
+        surfacePoint(V[v].World, F, h4, surf[b], rd, H, sp);
+        c = pixelAlbedo(sp);
+      }
       reinterpret_cast<float4*>(V[v].Linear)[b] = make_float4(c.x, c.y, c.z, 1.0f);
     }
   }
@@ -224,6 +238,41 @@ __global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) shadeVie
 #ifndef STRATUM_RESOLVE_OCC
 #define STRATUM_RESOLVE_OCC 0
 #endif
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, STRATUM_SHADE_OCC / THREADS) lightViewsK(const stratum_view* __restrict__ V,
+                                                                                int n, int grab, int order,
+                                                                                BatchScratch* S) {
+  const int lane = int(threadIdx.x & 31);
+  const int total = int(S->counters[kTotalTiles]);
+#pragma unroll 1
+  for (;;) {
+    const int t0 = claim(&S->counters[kLightNext], grab);
+    if (t0 >= total) break;
+    const int t1 = min(t0 + grab, total);
+#pragma unroll 1
+    for (int tile = t0; tile < t1; tile++) {
+      const int v = viewOf(V, n, tile);
+      const int W = V[v].width, H = V[v].height;
+      int tx, ty;
+      if (!tileCoord(tile - V[v].tileBase, V[v].tilesX, (H + kTileH - 1) / kTileH, order, tx, ty)) continue;
+      const int x = tx * kTileW + (lane & 7), y = ty * kTileH + (lane >> 3);
+      if (x >= W || y >= H) continue;
+      const size_t b = size_t(y) * W + x;
+      const float4 h4 = reinterpret_cast<const float4*>(V[v].Hit)[b];
+      if (int(h4.y) == kSkyId) continue;
+      const FrameConst F = S->view[v];
+      const f3 rd = primaryDir(F.cam, x, y, W, H);
+      float4* lin = reinterpret_cast<float4*>(V[v].Linear) + b;
+      const float4 a = *lin;
+      SurfacePoint sp;
+      surfacePoint(V[v].World, F, h4, reinterpret_cast<const float4*>(V[v].Surface)[b], rd, H, sp);
+      const f3 c = pixelLight(V[v].World, F, sp, rd, int(h4.y), mk(a.x, a.y, a.z));
+      *lin = make_float4(c.x, c.y, c.z, 1.0f);
+    }
+  }
+  retire(&S->counters[kLightNext], &S->counters[kLightDone], THREADS);
+}
+
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, STRATUM_RESOLVE_OCC / THREADS) resolveViewsK(const stratum_view* __restrict__ V, int n, int grab, int order,
                                                         BatchScratch* S) {
@@ -268,14 +317,16 @@ enum Parts { kTrace = 1, kShade = 2 };
 
 template <int T>
 int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratch* S, cudaStream_t s, int parts) {
-  static int traceGrid = 0, shadeGrid = 0, resolveGrid = 0;
+  static int traceGrid = 0, shadeGrid = 0, resolveGrid = 0, lightGrid = 0;
   if (!traceGrid) {
     traceGrid = residentBlocks(traceViewsK<T>, T, traceSmem(T));
     shadeGrid = residentBlocks(shadeViewsK<T>, T);
     resolveGrid = residentBlocks(resolveViewsK<T>, T);
+    lightGrid = residentBlocks(lightViewsK<T>, T);
   }
   if (parts & kTrace) traceViewsK<T><<<traceGrid, T, traceSmem(T), s>>>(V, n, t.grab, t.order, S);
   if (parts & kShade) shadeViewsK<T><<<shadeGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
+  if (parts & kShade) lightViewsK<T><<<lightGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
   if (parts & kShade) resolveViewsK<T><<<resolveGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
   return launchStatus();
 }

@@ -17,6 +17,8 @@ enum : int {
   kTotalTiles = 4,  // tiles over all views (written by the prologue)
   kResolveNext = 5,
   kResolveDone = 6,
+  kLightNext = 7,
+  kLightDone = 8,
   kCounters = 16
 };
 struct BatchScratch {

@@ -213,45 +213,69 @@ SD FrameConst makeFrame(const float* C, const uint32_t* O) {
   return f;
 }
 
-// Linear colour of one pixel (shade.cu:45-102).
-SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, float4 surf, f3 rd, int height) {
-  const f3 ro = F.cam.pos, sun = F.sun;
-  float t = hit.x;
-  int id = int(hit.y);
-  if (id == kSkyId) return skyColor(rd, sun);  // (a hit pixel's colour never reads the sky term)
-  f3 result;
-  f3 p = ro + rd * t, n = mk(surf.x, surf.y, surf.z);
-  int mat = int(hit.z), slot = int(surf.w);
-  if (slot >= kLots) slot = -1;  // never index past the table on a malformed Surface
-  float seed = hit.w;
+// Shading of one pixel (shade.cu:45-102) in three parts, so the batched path
+// can run the material and the lighting as two kernels (each a smaller body of
+// code for the instruction cache): the surface point, its albedo, its light.
+// shadePixel composes them; every path computes the same values in the same
+// order.
+
+// A hit pixel's surface as shading sees it (shade.cu:45-70): the hit point in
+// the world and lot frames, the normal (flipped for foliage seen from inside),
+// material and seed (ground: paving, asphalt or water from the lot), the
+// footprint and the masonry coordinates.
+struct SurfacePoint {
+  f3 p, n, q, qn;
   LotDesc lot;
-  f3 q = p, qn = n;
-  float palette = 0.0f;
+  int mat;
+  float seed, palette, t, sfp, u, v;
+};
+SD void surfacePoint(const float* __restrict__ W, const FrameConst& F, float4 hit, float4 surf, f3 rd, int height,
+                     SurfacePoint& s) {
+  s.t = hit.x;
+  s.p = F.cam.pos + rd * s.t;
+  s.n = mk(surf.x, surf.y, surf.z);
+  s.mat = int(hit.z);
+  int slot = int(surf.w);
+  if (slot >= kLots) slot = -1;  // never index past the table on a malformed Surface
+  s.seed = hit.w;
+  s.q = s.p; s.qn = s.n;
+  s.palette = 0.0f;
   if (slot >= 0) {
-    lot = loadLot(W, slot);
+    s.lot = loadLot(W, slot);
     int cx, cz;
     slotCell(F.o[0], F.o[2], slot, cx, cz);
-    f3 cp = mk(float(cx) * kCell, 0.0f, float(cz) * kCell) + mk(lot.ox, 0.0f, lot.oz);
-    q = toLot(p - cp, lot.turn);
-    qn = toLot(n, lot.turn);
-    palette = lot.palette;
+    f3 cp = mk(float(cx) * kCell, 0.0f, float(cz) * kCell) + mk(s.lot.ox, 0.0f, s.lot.oz);
+    s.q = toLot(s.p - cp, s.lot.turn);
+    s.qn = toLot(s.n, s.lot.turn);
+    s.palette = s.lot.palette;
   } else {  // ground: paving inside the lot, asphalt outside, water on canals
-    int cx = int(floorf((p.x + 18.0f) / kCell)), cz = int(floorf((p.z + 18.0f) / kCell));
+    int cx = int(floorf((s.p.x + 18.0f) / kCell)), cz = int(floorf((s.p.z + 18.0f) / kCell));
     slot = tableSlot(F.o[0], F.o[2], cx, cz);
-    lot = loadLot(W, slot);
-    q = p - mk(float(cx) * kCell, 0.0f, float(cz) * kCell);
-    seed = lot.seed;
-    mat = fabsf(q.x) < 16.5f && fabsf(q.z) < 16.5f ? 11 : 10;
-    if (lot.type == 5) mat = 9;
+    s.lot = loadLot(W, slot);
+    s.q = s.p - mk(float(cx) * kCell, 0.0f, float(cz) * kCell);
+    s.seed = s.lot.seed;
+    s.mat = fabsf(s.q.x) < 16.5f && fabsf(s.q.z) < 16.5f ? 11 : 10;
+    if (s.lot.type == 5) s.mat = 9;
   }
-  if (mat == 7 && dot(n, rd) > 0.0f) { n = n * -1.0f; qn = qn * -1.0f; }
-  float footprint = fmaxf(0.00005f, t * 1.08f / float(height));
-  float sfp = footprint / fmaxf(0.18f, fabsf(dot(n, rd)));
-  float u, v;
-  masonryUV(q, qn, u, v);
-  f3 base = substrateMean(mat);
-  if (mat == 0 || mat == 1) base = substrate(u, v, seed, mat);
-  f3 albedo = surfaceColor(q, qn, mat, seed, sfp, base) * paletteTint(palette, mat);
+  if (s.mat == 7 && dot(s.n, rd) > 0.0f) { s.n = s.n * -1.0f; s.qn = s.qn * -1.0f; }
+  float footprint = fmaxf(0.00005f, s.t * 1.08f / float(height));
+  s.sfp = footprint / fmaxf(0.18f, fabsf(dot(s.n, rd)));
+  masonryUV(s.q, s.qn, s.u, s.v);
+}
+// Material colour with the palette tint (materials.cu, shade.cu:71).
+SD f3 pixelAlbedo(const SurfacePoint& s) {
+  f3 base = substrateMean(s.mat);
+  if (s.mat == 0 || s.mat == 1) base = substrate(s.u, s.v, s.seed, s.mat);
+  return surfaceColor(s.q, s.qn, s.mat, s.seed, s.sfp, base) * paletteTint(s.palette, s.mat);
+}
+// Lighting of a hit pixel of this albedo (shade.cu:72-102): mortar relief
+// normal, sun shadow, ambient visibility, GGX, reflections, fog, debug views.
+SD f3 pixelLight(const float* __restrict__ W, const FrameConst& F, const SurfacePoint& s, f3 rd, int id, f3 albedo) {
+  const f3 sun = F.sun;
+  const f3 p = s.p, q = s.q, qn = s.qn;
+  const int mat = s.mat;
+  const float t = s.t, sfp = s.sfp, u = s.u, v = s.v, seed = s.seed;
+  f3 n = s.n, result;
   f3 originalN = n;
   if ((mat == 0 || mat == 1) && fabsf(qn.y) < 0.5f) {  // mortar relief normal by central differences
     float eps = fmaxf(0.002f, sfp * 0.6f);
@@ -265,7 +289,7 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
     f3 tangent = fabsf(qn.x) > 0.5f ? mk(0.0f, 0.0f, 1.0f) : mk(1.0f, 0.0f, 0.0f);
     float fade = freqWeight(sfp, 5.0f);
     f3 localN = unit(qn - tangent * (du * fade) - mk(0.0f, dv * fade, 0.0f));
-    n = fromLot(localN, lot.turn);
+    n = fromLot(localN, s.lot.turn);
   }
   if (mat == 9) n = unit(n + mk(cosf(q.x * 3.7f + q.z * 1.1f) * 0.06f, 0.0f, sinf(q.z * 4.4f - q.x * 0.9f) * 0.08f));
   float nl = fmaxf(0.0f, dot(n, sun)), nv = fmaxf(0.03f, -dot(n, rd));
@@ -305,13 +329,23 @@ SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, f
   fog = lerp(fog, 1.0f, smooth(kFar * 0.68f, kFar, t));
   f3 haze = skyColor(unit(mk(rd.x, 0.004f, rd.z)), sun);
   result = mix(result, haze, fog);
-  if (F.view == 1.0f) result = paletteTint(lot.palette, 0) * mk(0.4f, 0.55f, 0.6f);
+  if (F.view == 1.0f) result = paletteTint(s.lot.palette, 0) * mk(0.4f, 0.55f, 0.6f);
   if (F.view == 2.0f) {
     int g = id >= 0 ? id / kMaxFeatures : 0;
     result = mk(0.15f + 0.75f * hash1(g), 0.15f + 0.75f * hash1(g + 31), 0.15f + 0.75f * hash1(g + 98));
   }
   if (F.view == 3.0f) result = (n + mk(1.0f, 1.0f, 1.0f)) * 0.5f;
   return result;
+}
+
+
+// Linear colour of one pixel (shade.cu:45-102).
+SD f3 shadePixel(const float* __restrict__ W, const FrameConst& F, float4 hit, float4 surf, f3 rd, int height) {
+  const int id = int(hit.y);
+  if (id == kSkyId) return skyColor(rd, F.sun);  // (a hit pixel's colour never reads the sky term)
+  SurfacePoint s;
+  surfacePoint(W, F, hit, surf, rd, height, s);
+  return pixelLight(W, F, s, rd, id, pixelAlbedo(s));
 }
 
 SD float aces(float x) { return sat(x * (2.51f * x + 0.03f) / (x * (2.43f * x + 0.59f) + 0.14f)); }
