@@ -74,8 +74,8 @@ OPS_PER_RAY = {  # pose: (whole path, trace only)
 }
 # DRAM bytes per traced ray of traceViewsK: dram__bytes_read.sum +
 # dram__bytes_write.sum of one six-view 1600x900 launch (warm group cache, cold
-# L2 under ncu) = 133.0 MB + 226.6 MB over 8.64 M rays.
-TRACE_DRAM_BYTES_PER_RAY = 41.6
+# L2 under ncu) = 134.6 MB + 227.1 MB over 8.64 M rays.
+TRACE_DRAM_BYTES_PER_RAY = 41.9
 
 METRIC = "shaded rays/s @1600x900"
 
