@@ -738,6 +738,9 @@ def ours_arm(args):
                                                 args.serve_views, 3, tune_t),
             "sessions_64_at_1600x900": serve_poisson(200.0, 64, args.serve_seconds, (1600,), 150 << 30,
                                                      args.serve_views, 3, tune_t, seed=2),
+            # twice the offered load (580 M rays/s): headroom of the same 64 sessions
+            "sessions_64_at_1600x900_400rps": serve_poisson(400.0, 64, args.serve_seconds, (1600,), 150 << 30,
+                                                            args.serve_views, 3, tune_t, seed=4),
             # a budget that holds about two thirds of the sessions: LRU eviction and exact resumption at work
             "mixed_256_sessions_40gb_budget": serve_poisson(200.0, 256, args.serve_seconds, (768, 1024, 1600, 1920),
                                                             40 << 30, args.serve_views, 3, tune_t, seed=3),
