@@ -89,7 +89,7 @@ int stratum_resolveFrame(const float* Linear, float* History, unsigned* Pixels, 
 /* probeGrammar(Inputs[17], Output[16])                      kernels/probe.cu:2 */
 int stratum_probeGrammar(const float* Inputs, float* Output, stratum_stream_t stream);
 
-/* ---- north_star names of the same roles (legacy names of Stratum.cu) ------ */
+/* ---- page-oriented names of the same roles (legacy names of Stratum.cu) --- */
 /* initWorld = initCamera (Stratum.cu:95 role)                                   */
 int stratum_initWorld(float* C, unsigned* Origin, int seed, stratum_stream_t stream);
 /* schedulePages = clearQueue + prepareLots (Stratum.cu:172 role)                */

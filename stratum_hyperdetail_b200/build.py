@@ -5,8 +5,8 @@
 Steps: compile and run csrc/gen_tables.cpp (the grammar's trig constants,
 evaluated with the host C library) into _build/gen/trig_table.h, compile every
 csrc/*.cu and csrc/*.cpp with nvcc for sm_100a, link libstratum.so next to
-this file.  All device code is built with --fmad=false (see DESIGN.md,
-"Bit-exactness").
+this file.  All device code is built with --fmad=false: the reference's CPU
+build never fuses a multiply and an add, and its results are matched bit for bit.
 """
 from __future__ import annotations
 
