@@ -698,7 +698,7 @@ def ours_arm(args):
                 "path_frac": whole_ops / elapsed * world / world / peak,
                 "plain_trace_frac": trace_ops / (trace_plain.sum() * 1e-3) / peak}
     # the memory roofline of the same kernel, for contrast: its DRAM traffic per launch over the launch time
-    # against the pool's measured HBM copy bandwidth
+    # against the measured HBM copy bandwidth of this GPU model
     hbm_peak, hbm_src = 6650.0, "fallback 6.65 TB/s"
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     if peaks_file.exists():
