@@ -24,21 +24,28 @@ SD float nodeEntry(const float4* __restrict__ N, int node, f3 ro, f3 inv, float 
 }
 
 // Nearest hit inside one lot (trace.cu:8-28).  Returns true when a feature
-// nearer than `best` was found; then best/fid/feature are updated.
+// nearer than `best` was found; then best/fid/feature are updated.  Called only
+// once the lot's root entry was found nearer than `best` (trace.cu:53).
 SD bool queryLot(const LotDesc& lot, const float4* __restrict__ N, int slot, f3 ro, f3 rd, float cone, float& best,
                  int& fid, Feat& feature) {
   const f3 inv = invDir(rd);
   const int base = slot * kNodes;
   int stack[8], top = 0, node = 1, steps = 0;
   bool found = false;
+  // A node reached from its parent (or the root, tested by the caller) was
+  // found nearer than the same best a moment ago: the reference tests it again
+  // with the same result, so only nodes popped from the stack are re-tested.
+  bool fresh = true;
 #pragma unroll 1
   while (node > 0 && steps < kNodes) {
     steps++;
-    float nearT = nodeEntry(N, base + node, ro, inv, best);
-    if (nearT < best && node < kGroups) {
+    const bool near = fresh || nodeEntry(N, base + node, ro, inv, best) < best;
+    fresh = false;
+    if (near && node < kGroups) {
       int left = node * 2, right = left + 1;
       float ln = nodeEntry(N, base + left, ro, inv, best), rn = nodeEntry(N, base + right, ro, inv, best);
       bool lh = ln < best, rh = rn < best;
+      fresh = lh || rh;
       if (lh && rh) {
         int next = ln < rn ? left : right, other = ln < rn ? right : left;
         stack[top++] = other;  // at most one push per level of the 6-level tree
@@ -47,7 +54,7 @@ SD bool queryLot(const LotDesc& lot, const float4* __restrict__ N, int slot, f3 
       else if (rh) node = right;
       else { node = 0; if (top > 0) node = stack[--top]; }
     } else {
-      if (nearT < best && node >= kGroups) {
+      if (near && node >= kGroups) {
         HitSink s{ro, rd, cone, best, -1, Feat{}};
         runGroup(lot, node - kGroups, s);
         if (s.fid >= 0 && s.t < best) {
