@@ -100,9 +100,11 @@ def parse(argv=None):
     ap.add_argument("--serve-views", type=int, default=8, help="views per serving batch")
     ap.add_argument("--tune", default=None, help="threads,grab,order of the batched trace (default: autotune)")
     ap.add_argument("--random-views", type=int, default=64, help="views of the random multi-view scenario (0: skip)")
-    ap.add_argument("--streaming-frames", type=int, default=1000, help="frames of the streaming flight (0: skip)")
-    ap.add_argument("--streaming-check-every", type=int, default=10,
-                    help="frames between hierarchy-vs-exhaustive checks of 65,536 random rays")
+    ap.add_argument("--streaming-frames", type=int, default=15000,
+                    help="frames of the streaming flight (15,000 = 10 km at 40 m/s and 60 Hz; 0: skip)")
+    ap.add_argument("--streaming-check-every", type=int, default=54,
+                    help="frames between hierarchy-vs-exhaustive checks of 65,536 random rays "
+                         "(54 frames = one 36 m cell at 40 m/s)")
     a = ap.parse_args(argv)
     a.poses = [p for p in a.poses.split(",") if p]
     if a.tune:
@@ -247,6 +249,23 @@ class ClockSampler:
                 "samples": len(sm), "source": self.source}
 
 
+def random_view_specs(n_views, seed=1):
+    """The multi-view workload's views, in draw order: (samples, width, height,
+    world seed, origin (xl, xh, zl, zh), pos, yaw, pitch) from a counter-based
+    PRNG (Philox) seeded `seed`."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    specs = []
+    for _ in range(n_views):
+        w = int(round(320 * 6 ** rng.random()))
+        h = int(round(w * 9 / 16))
+        origin = [int(x) for x in rng.integers(0, 2**32, size=4, dtype=np.uint64)]
+        pos = (float(rng.uniform(-18, 18)), float(rng.uniform(1.5, 300.0)), float(rng.uniform(-18, 18)))
+        yaw, pitch = math.radians(rng.uniform(0, 360)), math.radians(rng.uniform(-45, 10))
+        seed_w, samples = int(rng.integers(0, 1 << 24)), int(rng.integers(1, 65))
+        specs.append((samples, w, h, seed_w, origin, pos, yaw, pitch))
+    return specs
+
+
 def random_views(n_views, tune, steps=1, warmup=1):
     """Batched multi-view scenario: `n_views` independent views drawn from a
     counter-based PRNG (Philox) seeded 1 -- 16:9 with width log-uniform in
@@ -264,17 +283,7 @@ def random_views(n_views, tune, steps=1, warmup=1):
     import stratum_hyperdetail_b200 as sb
     from stratum_hyperdetail_b200.batch import Batch
     from stratum_hyperdetail_b200.views import View
-    rng = np.random.Generator(np.random.Philox(1))
-    specs = []
-    for _ in range(n_views):
-        w = int(round(320 * 6 ** rng.random()))
-        h = int(round(w * 9 / 16))
-        origin = [int(x) for x in rng.integers(0, 2**32, size=4, dtype=np.uint64)]
-        pos = (float(rng.uniform(-18, 18)), float(rng.uniform(1.5, 300.0)), float(rng.uniform(-18, 18)))
-        yaw, pitch = math.radians(rng.uniform(0, 360)), math.radians(rng.uniform(-45, 10))
-        seed, samples = int(rng.integers(0, 1 << 24)), int(rng.integers(1, 65))
-        specs.append((samples, w, h, seed, origin, pos, yaw, pitch))
-    specs.sort(key=lambda s: -s[0])
+    specs = sorted(random_view_specs(n_views), key=lambda s: -s[0])
     views = []
     for samples, w, h, seed, origin, pos, yaw, pitch in specs:
         v = View(w, h)
@@ -338,16 +347,19 @@ def streaming(frames, check_every, tune, rays_per_check=65536):
     """Streaming-world scenario: one 1024x576 view flies straight along +x at
     40 m/s and 40 m altitude, 60 Hz simulated time, from lot address
     xl = 0xFFFFFFF0 (so the 64-bit carry into xh is crossed after 16 lots, at
-    frame 837).  Each frame is one batched frame call: stepCamera, refresh of the
-    lots that entered the 128x128 table (one 128-lot column per 36 m cell),
-    rebuild of their hierarchies, trace, shade and resolve.  Every
-    `check_every` frames, 65,536 uniformly random rays (Philox seeded 1: origins
-    uniform over the table's +-1 km square at 0.5-100 m, directions uniform on
-    the sphere) are traced through the hierarchy and exhaustively (every group
-    of every visited lot) and compared bit for bit; checks are outside the
-    frame timing."""
+    frame 837); 15,000 frames are the 10 km flight (278 cells).  Each frame is
+    one batched frame call: stepCamera, refresh of the lots that entered the
+    128x128 table (one 128-lot column per 36 m cell), rebuild of their
+    hierarchies, trace, shade and resolve.  Every `check_every` frames, 65,536
+    uniformly random rays (Philox seeded 1: origins uniform over the table's
+    +-1 km square at 0.5-100 m, directions uniform on the sphere) are traced
+    through the hierarchy and exhaustively (every group of every visited lot):
+    distances must agree bit for bit, and where the two name different
+    features both are re-tested on the ray (stratum_retestFeatures) -- equal
+    distances bit for bit are an exact tie, the rest are counted as
+    `identity_mismatches_non_tie`.  Checks are outside the frame timing."""
     import torch
-    import stratum_hyperdetail_b200 as sb
+    import stratum_hyperdetail_b200.rays as sr
     from stratum_hyperdetail_b200.batch import Batch
     from stratum_hyperdetail_b200.views import View
     v = View(1024, 576)
@@ -358,11 +370,11 @@ def streaming(frames, check_every, tune, rays_per_check=65536):
     b.set_dt(1.0 / 60.0)
     rng = np.random.Generator(np.random.Philox(1))
     stream = torch.cuda.current_stream()
-    s = stream.cuda_stream
-    out_h = torch.empty(rays_per_check * 8, dtype=torch.float32, device="cuda")
+    out_h = torch.empty((rays_per_check, 8), dtype=torch.float32, device="cuda")
     out_e = torch.empty_like(out_h)
     ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-    marks, checks, bad_t, bad_id, check_ms = [], 0, 0, 0, 0.0
+    marks, checks, check_ms = [], 0, 0.0
+    tally = {"distance_mismatches": 0, "identity_mismatches": 0, "identity_ties": 0, "identity_mismatches_non_tie": 0}
     for f in range(frames):
         a, c = ev(), ev()
         a.record(stream)
@@ -377,16 +389,13 @@ def streaming(frames, check_every, tune, rays_per_check=65536):
             rays = torch.from_numpy(np.concatenate([ro, d, np.full((n, 1), 0.0015)], 1).astype(np.float32)).cuda()
             x, y = ev(), ev()
             x.record(stream)
-            sb.call("stratum_traceRays", sb.ptr(v.World), sb.ptr(v.Nodes), sb.ptr(v.Origin), sb.ptr(rays), n, 0,
-                    sb.ptr(out_h), s)
-            sb.call("stratum_traceRays", sb.ptr(v.World), sb.ptr(v.Nodes), sb.ptr(v.Origin), sb.ptr(rays), n, 1,
-                    sb.ptr(out_e), s)
+            sr.trace(v, rays, False, out_h, stream)
+            sr.trace(v, rays, True, out_e, stream)
             y.record(stream)
             y.synchronize()
             check_ms += x.elapsed_time(y)
-            hb, eb = out_h.view(torch.int32).view(-1, 8), out_e.view(torch.int32).view(-1, 8)
-            bad_t += int((hb[:, 0] != eb[:, 0]).sum())
-            bad_id += int((hb[:, 1] != eb[:, 1]).sum())
+            for k, val in sr.compare_hierarchy(v, rays, out_h, out_e, stream).items():
+                tally[k] += val
             checks += 1
     torch.cuda.synchronize()
     fm = np.array([a.elapsed_time(c) for a, c in marks])
@@ -395,8 +404,8 @@ def streaming(frames, check_every, tune, rays_per_check=65536):
            "frame_ms_mean": float(fm.mean()), "frame_ms_p99": float(np.percentile(fm, 99)),
            "frames_per_s": 1e3 / float(fm.mean()), "rays_per_s": 1024 * 576 / (float(fm.mean()) * 1e-3),
            "final_origin": [int(x) for x in org], "carry_crossed": bool(org[1] == 1),
-           "checks": checks, "rays_checked": checks * rays_per_check, "distance_mismatches": bad_t,
-           "identity_mismatches": bad_id, "check_ms_mean": check_ms / max(checks, 1)}
+           "checks": checks, "rays_checked": checks * rays_per_check, **tally,
+           "check_ms_mean": check_ms / max(checks, 1)}
     del b, v
     torch.cuda.synchronize()
     torch.cuda.empty_cache()

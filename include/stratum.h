@@ -127,6 +127,14 @@ int stratum_featureQuery(const float* Queries, int n, float* Results, stratum_st
  * be NULL): the check of the hierarchy (tests/native_harness.cpp:68-79). */
 int stratum_traceRays(const float* World, const float* Nodes, const unsigned* Origin, const float* Rays, int n,
                       int exhaustive, float* Out, stratum_stream_t stream);
+/* One named feature per ray: Ids n x 2 i32 [slot, fid] (a traced ray's Out[7]
+ * and Out[1]) -> Out n x 4 f32 [t, normal.xyz], the feature regenerated from
+ * the slot's descriptor and intersected in its lot frame as the trace does
+ * (kernels/world.cu:37-56, kernels/sink.cu:21, kernels/geometry.cu:33,92);
+ * t = 2000 where the ray misses it.  Two ids of one ray that give the same t bit
+ * for bit are an exact tie: either is a correct nearest hit. */
+int stratum_retestFeatures(const float* World, const unsigned* Origin, const float* Rays, const int* Ids, int n,
+                           float* Out, stratum_stream_t stream);
 
 /* ---- batched views (no reference counterpart: B200 multi-view form) ------- */
 /* One view of a batch: device pointers to that view's own buffers, in the

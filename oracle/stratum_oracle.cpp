@@ -1263,6 +1263,112 @@ void resolvePixel(const float* Lin, float* Hist, uint32_t* Px, const float* C, c
 
 int useThreads(int n) { return n > 0 ? n : omp_get_max_threads(); }
 
+// ---- FP64 re-intersection of a pixel's winning feature ----------------------
+// The error bound of a traced frame: the feature a pixel's Hit names is
+// regenerated from its lot descriptor (group fid/64, record fid%64, the
+// emission of assets.cu:3-265), the pixel's float primary ray (common.cu:63-70)
+// is moved into that lot's frame in double precision (trace.cu:49-50), and the
+// feature is intersected again by hitFeature<double> (geometry.cu:33-91), its
+// normal taken by featNormal<double> (geometry.cu:92-114) at the FP64 hit and,
+// to check the normal function apart from the distance, at the float path's
+// own hit point.
+//
+// Foliage (material 7 ellipsoids) is a DDA over leaf discs whose cell sequence
+// can differ at a cell boundary in FP64, so the "same feature" there is the
+// leaf disc: the 3x3x3 cells around the float hit point are searched for a
+// disc of the envelope (geometry.cu:17-26) that the ray crosses in FP64, the
+// one nearest the float distance is taken, and its FP64 plane intersection
+// and normal are returned.
+// Ground hits (fid -1) re-intersect the plane y = 0 (trace.cu:34).
+// status = kind | shape << 3 | material << 8 (shape and material of a feature).
+enum { RX_SKY = 0, RX_GROUND = 1, RX_FEATURE = 2, RX_LEAF = 3, RX_MISSED = 4 };
+
+static int leafReintersect(const Feat& f, V3<double> ro, V3<double> rd, V3f hitPoint, double tFloat, double& t64,
+                           V3<double>& n64) {
+  const double cell = double(0.18f);
+  const V3<double> centre = cast3<double>(f.p), radius = cast3<double>(f.h);
+  const int bx = int(std::floor(hitPoint.x / 0.18f)), by = int(std::floor(hitPoint.y / 0.18f)),
+            bz = int(std::floor(hitPoint.z / 0.18f));
+  const int seed = int(f.seed);
+  double bestGap = 1e30;
+  int found = 0;
+  for (int dz = -1; dz <= 1; dz++)
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const int ix = bx + dx, iy = by + dy, iz = bz + dz;
+        V3<double> c = mk((double(ix) + 0.5) * cell, (double(iy) + 0.5) * cell, (double(iz) + 0.5) * cell);
+        V3<double> q = c - centre;
+        double ell = q.x * q.x / (radius.x * radius.x) + q.y * q.y / (radius.y * radius.y) +
+                     q.z * q.z / (radius.z * radius.z);
+        if (!(ell < 1.0 && hash2(ix + iy * 113, iz, seed) > 0.20f)) continue;
+        V3<double> n = leafNormal<double>(ix, iy, iz, seed);
+        double den = dot(rd, n);
+        if (std::fabs(den) <= 1e-5) continue;
+        double u = dot(c - ro, n) / den;
+        V3<double> pp = ro + rd * u - c;
+        V3<double> tangent = unit(cross(n, mk(0.0, 0.0, 1.0)));
+        V3<double> bitangent = cross(n, tangent);
+        double a = dot(pp, tangent) / double(0.125f), b = dot(pp, bitangent) / double(0.062f);
+        if (!(a * a + b * b < 1.0)) continue;
+        double gap = std::fabs(u - tFloat);
+        if (gap < bestGap) { bestGap = gap; t64 = u; n64 = n; found = 1; }
+      }
+  return found;
+}
+
+static void reintersectPixel(const float* W, const uint32_t* O, const float* C, const float* Hit, const float* Surf,
+                             int width, int height, int x, int y, double* t64, double* n64, int32_t* status) {
+  const size_t p = size_t(y) * width + x, b = p * 4;
+  const int fid = int(Hit[b + 1]), slot = int(Surf[b + 3]);
+  V3f rof = camPos(C), rdf = primaryDir(C, x, y, width, height);
+  V3<double> ro = cast3<double>(rof), rd = cast3<double>(rdf);
+  t64[p] = double(kFar);
+  for (int k = 0; k < 6; k++) n64[p * 6 + k] = k % 3 == 1 ? 1.0 : 0.0;
+  if (fid == -1) {
+    t64[p] = -ro.y / rd.y;
+    status[p] = RX_GROUND;
+    return;
+  }
+  if (fid < 0 || slot < 0 || slot >= kLots) { status[p] = RX_SKY; return; }
+  const LotDesc lot = loadLot(W, slot);
+  const int group = fid / kMaxFeatures, index = fid % kMaxFeatures;
+  Feat f{mk(0.f, 0.f, 0.f), mk(1.f, 1.f, 1.f), -1, 0, 0, 0.0f};
+  forEachFeature(lot, group, [&](const Feat& ft, int id) { if (id == index) f = ft; });
+  const int32_t kind = ((f.shape & 15) << 3) | (f.material << 8);
+  int cx, cz;
+  slotCell(O, slot, cx, cz);
+  const V3<double> cp = mk(double(cx) * double(kCell) + double(lot.ox), 0.0, double(cz) * double(kCell) + double(lot.oz));
+  const V3<double> lr = toLot(ro - cp, lot.turn), ld = toLot(rd, lot.turn);
+  // the float path's lot-frame ray, exactly as the trace forms it
+  const V3f cpf = mk(float(cx) * kCell + lot.ox, 0.0f, float(cz) * kCell + lot.oz);
+  const V3f lrf = toLot(rof - cpf, lot.turn), ldf = toLot(rdf, lot.turn);
+  if (f.shape == 1 && f.material == 7) {
+    const float tf = Hit[b];
+    V3<double> n;
+    double t;
+    if (leafReintersect(f, lr, ld, lrf + ldf * tf, double(tf), t, n)) {
+      t64[p] = t;
+      n = fromLot(n, lot.turn);
+      n64[p * 6] = n.x; n64[p * 6 + 1] = n.y; n64[p * 6 + 2] = n.z;
+      n64[p * 6 + 3] = n.x; n64[p * 6 + 4] = n.y; n64[p * 6 + 5] = n.z;
+      status[p] = RX_LEAF | kind;
+    } else {
+      status[p] = RX_MISSED | kind;
+    }
+    return;
+  }
+  const double cone = double(1.08f / float(height));
+  const double t = hitFeature<double>(f, lr, ld, cone, nullptr);
+  if (!(t < double(kFar))) { status[p] = RX_MISSED | kind; return; }
+  const V3<double> n = fromLot(featNormal<double>(f, lr + ld * t), lot.turn);
+  t64[p] = t;
+  n64[p * 6] = n.x; n64[p * 6 + 1] = n.y; n64[p * 6 + 2] = n.z;
+  // the normal function alone: featNormal in FP64 at the float path's own hit point
+  const V3<double> nf = fromLot(featNormal<double>(f, cast3<double>(lrf + ldf * Hit[b])), lot.turn);
+  n64[p * 6 + 3] = nf.x; n64[p * 6 + 4] = nf.y; n64[p * 6 + 5] = nf.z;
+  status[p] = RX_FEATURE | kind;
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -1462,6 +1568,38 @@ void orc_traceRays(const float* W, const float* N, const uint32_t* O, const floa
     const float* q = rays + size_t(i) * 7;
     traceRayOrc(W, N, O, mk(q[0], q[1], q[2]), mk(q[3], q[4], q[5]), q[6], exhaustive != 0, out + size_t(i) * 8);
   }
+}
+// One named (slot, fid) feature per ray, intersected in its lot frame as the
+// trace forms it (world.cu:37-56, sink.cu:21, geometry.cu:33-114).
+void orc_retestFeatures(const float* W, const uint32_t* O, const float* rays, const int32_t* ids, int n, float* out,
+                        int nthreads) {
+#pragma omp parallel for schedule(dynamic, 64) num_threads(useThreads(nthreads))
+  for (int i = 0; i < n; i++) {
+    const float* q = rays + size_t(i) * 7;
+    const int slot = ids[2 * i], fid = ids[2 * i + 1];
+    float* o = out + size_t(i) * 4;
+    o[0] = kFar; o[1] = o[2] = o[3] = 0.0f;
+    if (slot < 0 || slot >= kLots || fid < 0 || fid >= kGroups * kMaxFeatures) continue;
+    const LotDesc lot = loadLot(W, slot);
+    int cx, cz;
+    slotCell(O, slot, cx, cz);
+    const V3f ro = mk(q[0], q[1], q[2]), rd = mk(q[3], q[4], q[5]);
+    const V3f cp = mk(float(cx) * kCell + lot.ox, 0.0f, float(cz) * kCell + lot.oz);
+    const V3f lr = toLot(ro - cp, lot.turn), ld = toLot(rd, lot.turn);
+    Feat f{mk(0.f, 0.f, 0.f), mk(1.f, 1.f, 1.f), -1, 0, 0, 0.0f};
+    forEachFeature(lot, fid / kMaxFeatures, [&](const Feat& ft, int id) { if (id == fid % kMaxFeatures) f = ft; });
+    if (f.shape < 0) continue;
+    const float t = hitFeature<float>(f, lr, ld, q[6], nullptr);
+    if (!(t > 0.001f && t < kFar)) continue;
+    const V3f nn = fromLot(featNormal<float>(f, lr + ld * t), lot.turn);
+    o[0] = t; o[1] = nn.x; o[2] = nn.y; o[3] = nn.z;
+  }
+}
+void orc_reintersectF64(const float* W, const uint32_t* O, const float* C, const float* Hit, const float* Surf,
+                        int width, int height, double* t64, double* n64, int32_t* status, int nthreads) {
+#pragma omp parallel for schedule(dynamic, 2) num_threads(useThreads(nthreads))
+  for (int y = 0; y < height; y++)
+    for (int x = 0; x < width; x++) reintersectPixel(W, O, C, Hit, Surf, width, height, x, y, t64, n64, status);
 }
 void orc_resolveRows(const float* Lin, float* Hist, uint32_t* Px, const float* C, const float* Hit, const float* Surf,
                      int width, int height, int rowStart, int rowCount, int nthreads) {

@@ -77,6 +77,19 @@ void orc_traceRays(const float* World, const float* Nodes, const uint32_t* Origi
 void orc_resolveRows(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
                      const float* Surface, int width, int height, int rowStart, int rowCount, int nthreads);
 void orc_probeGrammar(const float* Inputs, float* Output);
+/* rays n x 7 as orc_traceRays; ids n x 2 [slot, fid]; out n x 4 [t, n.xyz] of
+ * that one feature on that ray (t = 2000 if missed). */
+void orc_retestFeatures(const float* World, const uint32_t* Origin, const float* rays, const int32_t* ids, int n,
+                        float* out, int nthreads);
+/* FP64 re-intersection of every pixel's winning feature, given a frame's
+ * World/Origin/C and its Hit/Surface: t64 (P), n64 (P x 6, world frame: the
+ * normal at the FP64 hit, then at the frame's own float hit point) and a
+ * status per pixel: 0 sky, 1 ground plane, 2 feature, 3 foliage leaf disc,
+ * 4 not re-found in FP64, in bits 0-2; the feature's shape in bits 3-6 and
+ * its material from bit 8. */
+void orc_reintersectF64(const float* World, const uint32_t* Origin, const float* C, const float* Hit,
+                        const float* Surface, int width, int height, double* t64, double* n64, int32_t* status,
+                        int nthreads);
 
 #ifdef __cplusplus
 }

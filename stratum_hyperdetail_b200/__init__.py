@@ -69,6 +69,7 @@ SIGNATURES: dict[str, list] = {
     "stratum_enumerateGroups": [_P, _P, _I, _I, _P, _P, _S],
     "stratum_featureQuery": [_P, _I, _P, _S],
     "stratum_traceRays": [_P, _P, _P, _P, _I, _I, _P, _S],
+    "stratum_retestFeatures": [_P, _P, _P, _P, _I, _P, _S],
     "stratum_applyPoses": [_P, _P, _P, _I, _S],
     "stratum_stepViews": [_P, _I, _S],
     "stratum_refreshViews": [_P, _I, _S],

@@ -71,9 +71,50 @@ __global__ void __launch_bounds__(64) traceRaysK(const float* __restrict__ W, co
   o[1] = make_float4(r.normal.x, r.normal.y, r.normal.z, float(r.slot));
 }
 
+// One named feature of a table against one ray: the lot of `slot` (its
+// descriptor, cell and turn, kernels/world.cu:37-56), record fid % 64 of group
+// fid / 64 (the enumeration sink of kernels/sink.cu:21), intersected in that
+// lot's frame exactly as the trace forms it (kernels/trace.cu:49-50).
+// Out: [t, normal.xyz] (t = FAR if the ray misses it or the id names nothing).
+__global__ void __launch_bounds__(64) retestFeaturesK(const float* __restrict__ W, const uint32_t* __restrict__ O,
+                                                     const float* __restrict__ rays, const int* __restrict__ ids,
+                                                     int n, float* out) {
+  int i = int(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= n) return;
+  const float* q = rays + size_t(i) * 7;
+  const int slot = ids[2 * i], fid = ids[2 * i + 1];
+  float4 r = make_float4(kFar, 0.0f, 0.0f, 0.0f);
+  if (slot >= 0 && slot < kLots && fid >= 0 && fid < kGroups * kMaxFeatures) {
+    const LotDesc lot = loadLot(W, slot);
+    int cx, cz;
+    slotCell(O[0], O[2], slot, cx, cz);
+    const f3 ro = mk(q[0], q[1], q[2]), rd = mk(q[3], q[4], q[5]);
+    const f3 cp = mk(float(cx) * kCell + lot.ox, 0.0f, float(cz) * kCell + lot.oz);
+    const f3 lr = toLot(ro - cp, lot.turn), ld = toLot(rd, lot.turn);
+    PickSink pick{fid % kMaxFeatures};
+    runGroup(lot, fid / kMaxFeatures, pick);
+    if (pick.f.shape >= 0) {
+      const float t = featureHitCall(pick.f, lr, ld, q[6]);
+      if (t > 0.001f && t < kFar) {
+        const f3 nn = fromLot(featureNormal(pick.f, lr + ld * t), lot.turn);
+        r = make_float4(t, nn.x, nn.y, nn.z);
+      }
+    }
+  }
+  reinterpret_cast<float4*>(out)[i] = r;
+}
+
 }  // namespace st
 
 using namespace st;
+
+extern "C" int stratum_retestFeatures(const float* World, const unsigned* Origin, const float* Rays, const int* Ids,
+                                      int n, float* Out, stratum_stream_t stream) {
+  if (!World || !Origin || !Rays || !Ids || !Out || n < 0) return STRATUM_EINVAL;
+  if (n == 0) return STRATUM_OK;
+  retestFeaturesK<<<(n + 63) / 64, 64, 0, asStream(stream)>>>(World, Origin, Rays, Ids, n, Out);
+  return launchStatus();
+}
 
 extern "C" int stratum_traceRays(const float* World, const float* Nodes, const unsigned* Origin, const float* Rays,
                                  int n, int exhaustive, float* Out, stratum_stream_t stream) {

@@ -143,6 +143,8 @@ class Oracle(_Lib):
         L.orc_featureNormal_f64.argtypes = [f32p, f64p, f64p]
         L.orc_queryLot_exhaustive.restype = ct.c_float
         L.orc_queryLot_exhaustive.argtypes = [f32p, f32p, f32p, ct.c_float, ct.c_float, ct.POINTER(ct.c_int), f32p]
+        L.orc_retestFeatures.argtypes = [f32p, u32p, f32p, i32p, ct.c_int, f32p, ct.c_int]
+        L.orc_reintersectF64.argtypes = [f32p, u32p, f32p, f32p, f32p, ct.c_int, ct.c_int, f64p, f64p, i32p, ct.c_int]
 
     def build_bounds(self, queue, world, nodes, nthreads=0):
         self.lib.orc_buildBounds(queue, world, nodes, nthreads)
@@ -181,6 +183,28 @@ class Oracle(_Lib):
         out = np.zeros(3, np.float64)
         self.lib.orc_featureNormal_f64(np.ascontiguousarray(f10, np.float32), np.ascontiguousarray(pt, np.float64), out)
         return out
+
+    def retest_features(self, world, origin, rays, ids, nthreads=0):
+        """[t, n.xyz] of feature ids[i] = (slot, fid) on ray i, in its lot frame as the trace forms it."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        ids = np.ascontiguousarray(ids, np.int32)
+        out = np.zeros((len(rays), 4), np.float32)
+        self.lib.orc_retestFeatures(world, np.ascontiguousarray(origin, np.uint32), rays, ids, len(rays), out, nthreads)
+        return out
+
+    def reintersect_f64(self, world, origin, C, hit, surface, w, h, nthreads=0):
+        """FP64 re-intersection of every pixel's winning feature: (t64 [P], n64 [P, 6], status [P]).
+        n64[:, :3] is the normal at the FP64 hit, n64[:, 3:] the FP64 normal at the frame's float hit point.
+        status & 7: 0 sky, 1 ground, 2 feature, 3 foliage leaf disc, 4 not re-found in FP64;
+        (status >> 3) & 15: the feature's shape; status >> 8: its material."""
+        P = w * h
+        t64 = np.zeros(P, np.float64)
+        n64 = np.zeros(P * 6, np.float64)
+        st = np.zeros(P, np.int32)
+        self.lib.orc_reintersectF64(world, np.ascontiguousarray(origin, np.uint32), np.ascontiguousarray(C, np.float32),
+                                    np.ascontiguousarray(hit, np.float32), np.ascontiguousarray(surface, np.float32),
+                                    int(w), int(h), t64, n64, st, nthreads)
+        return t64, n64.reshape(P, 6), st
 
     def query_lot_exhaustive(self, lot16, ro, rd, best=FAR, cone=0.0):
         fid = ct.c_int(0)

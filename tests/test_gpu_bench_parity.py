@@ -1,0 +1,254 @@
+"""The benchmarked workloads against the CPU oracle, through the C ABI.
+
+The six poses of the 1600x900 workload (bench.POSES, seed 0x5EED) are rendered
+as whole frames at samples 1, 2, 7 and 64 -- samples after the first take the
+Halton(2,3) jitter of kernels/common.cu:58-70, and History holds a running
+mean with count > 1 (kernels/shade.cu:115-118; at sample 64 half the pixels
+are already converged and must stay frozen) -- on three paths:
+
+* the drop-in entry points in the reference's launch structure (64-row
+  tracePrimary / shadePixels strips, then resolveFrame);
+* the batched renderer, all six views in one launch per kernel (eager);
+* the batched frame captured as a CUDA graph and replayed (the bench's timed
+  path: stepViews advances the sample, then refresh, build and render).
+
+Each is compared with the oracle's frame of the same pose and sample:
+identity (lot, group, feature) on every ray whose two nearest candidates are
+farther apart than the distance tolerance, distance and normal within 1e-5
+relative, material and seed exact, Linear and History within 1/1024 per
+channel with the mismatches counted and printed.  The two batched paths must
+equal the drop-in path bit for bit.
+
+The drop-in frame's winning features are also re-intersected in FP64 (the
+oracle's hitFeature<double>/featNormal<double> on the pixel's float ray): the
+distance within 1e-5 relative on the well-conditioned shapes (ground, boxes,
+prisms, leaf discs), the normal function within 1e-5 at the frame's own hit
+point on every shape, and the float quadratics of ellipsoids, cylinders,
+arches and rings reported with their error distribution (their precision is
+that of the reference's float formulation, which the GPU reproduces bit for
+bit).
+
+Eight views of the multi-view workload (bench.random_view_specs: random 64-bit
+addresses, world seeds, sizes, poses and sample counts) are checked the same
+way, batched in one launch and through the drop-in strips.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle_lib as ol
+from bench import HEIGHT, POSES, SEED, WIDTH, random_view_specs
+from gpu_lib import compare_frames
+
+pytestmark = pytest.mark.gpu
+TOL_T, TOL_N, TOL_C = 1e-5, 1e-5, 1.0 / 1024.0
+SAMPLES = (1, 2, 7, 64)
+ROWS = 64
+KEYS = ("Hit", "Surface", "Linear", "History", "Pixels")
+
+
+def seeded_history(P, k, seed):
+    """A History buffer as it stands before sample k: random colour, count k-1
+    (at k = 64 every second pixel already holds 64 samples and is frozen)."""
+    rng = np.random.default_rng(seed)
+    h = rng.random((P, 4), dtype=np.float32)
+    h[:, 3] = float(max(k - 1, 0))
+    if k >= 64:
+        h[::2, 3] = 64.0
+    return h.reshape(-1)
+
+
+def drop_in(v, sb):
+    """trace and shade in 64-row strips, then resolve (src/engine.js:76-78)."""
+    call, P, s = sb.call, sb.ptr, torch.cuda.current_stream().cuda_stream
+    w, h = v.width, v.height
+    for y in range(0, h, ROWS):
+        call("stratum_tracePrimary", P(v.World), P(v.Nodes), P(v.Origin), P(v.C), P(v.Hit), P(v.Surface), w, h, y,
+             min(ROWS, h - y), s)
+    for y in range(0, h, ROWS):
+        call("stratum_shadePixels", P(v.World), P(v.Origin), P(v.C), P(v.Hit), P(v.Surface), P(v.Linear), w, h, y,
+             min(ROWS, h - y), s)
+    call("stratum_resolveFrame", P(v.Linear), P(v.History), P(v.Pixels), P(v.C), P(v.Hit), P(v.Surface), w, h, s)
+
+
+def arm(views, hist, samples):
+    """Put view i at sample samples[i] with its seeded History."""
+    for v, hh, k in zip(views, hist, samples):
+        v.C[19] = float(k)
+        v.History.copy_(torch.from_numpy(hh))
+
+
+def grab(v):
+    return {key: getattr(v, key).clone() for key in KEYS}
+
+
+def host(frame):
+    out = {key: frame[key].cpu().numpy() for key in KEYS}
+    out["Pixels"] = out["Pixels"].view(np.uint32)
+    return out
+
+
+def same_bits(a, b):
+    return all(np.array_equal(a[k].view(np.uint32), b[k].view(np.uint32)) for k in KEYS)
+
+
+def fp64_report(orc, o, frame, w, h):
+    """Per-class counts of the frame's distances and normals beyond 1e-5 of the
+    FP64 re-intersection of the same feature.  `missed`: pixels whose feature
+    the FP64 computation does not hit at all (grazing float hits)."""
+    hit, surf = frame["Hit"], frame["Surface"]
+    t64, n64, st = orc.reintersect_f64(o.World, o.Origin, o.C, hit, surf, w, h)
+    kind, shape, mat = st & 7, (st >> 3) & 15, st >> 8
+    t = hit.reshape(-1, 4)[:, 0].astype(np.float64)
+    n = surf.reshape(-1, 4)[:, :3].astype(np.float64)
+    rel = np.abs(t - t64) / np.maximum(t64, 1e-6)
+    n_same = np.abs(n - n64[:, 3:]).max(axis=1)
+    n_fp64 = np.abs(n - n64[:, :3]).max(axis=1)
+    feat = (kind >= 2) & (kind <= 4)
+    found = kind != 4
+    leaf = feat & (shape == 1) & (mat == 7)
+    classes = {
+        "ground": kind == 1,
+        "box": feat & (shape == 0),
+        "prism": feat & (shape == 3),
+        "leaf": leaf,
+        "arch": feat & (shape == 4),
+        "ellipsoid": feat & (shape == 1) & ~leaf,
+        "cylinder": feat & (shape == 2),
+        "ring": feat & (shape == 7),
+    }
+    rep = {"pixels_hit": int((kind >= 1).sum())}
+    for name, m in classes.items():
+        f = m & found
+        rep[name] = {"n": int(m.sum()), "missed": int((m & ~found).sum()),
+                     "t_beyond": int((f & (rel > TOL_T)).sum()),
+                     "normal_fn_beyond": int((f & (n_same > TOL_N)).sum()),
+                     "normal_at_fp64_hit_beyond": int((f & (n_fp64 > TOL_N)).sum()),
+                     "t_p999": float(np.percentile(rel[f], 99.9)) if f.any() else 0.0,
+                     "t_max": float(rel[f].max()) if f.any() else 0.0}
+    return rep
+
+
+def check_fp64(rep):
+    """Well-conditioned shapes: distance within 1e-5 of FP64 (and re-found) on
+    all but 1e-4 of their pixels.  Every shape: the normal function within 1e-5
+    at the frame's own hit point on all but 1e-4.  The float quadratics
+    (arches, ellipsoids, cylinders, rings) lose digits when the ray origin is
+    many radii away -- the reference's formulation, reproduced bit for bit --
+    so they are reported, with a ceiling that catches a wrong root."""
+    classes = [c for c in rep if isinstance(rep[c], dict)]
+    well = ("ground", "box", "prism", "leaf")
+    n_well = sum(rep[c]["n"] for c in well)
+    assert sum(rep[c]["t_beyond"] + rep[c]["missed"] for c in well) <= max(2, n_well * 1e-4), rep
+    n_all = sum(rep[c]["n"] for c in classes)
+    assert sum(rep[c]["normal_fn_beyond"] for c in classes) <= max(2, n_all * 1e-4), rep
+    for c in ("arch", "ellipsoid", "cylinder", "ring"):
+        assert rep[c]["t_p999"] <= 1e-2, (c, rep[c])
+
+
+def check_against_oracle(tag, got, want, second):
+    rep = compare_frames(got, want, second, TOL_T, TOL_N, TOL_C)
+    print(tag, {k: rep[k] for k in ("rays", "identity_mismatch", "identity_bad", "t_bad", "n_bad", "material_bad",
+                                     "linear_bad", "linear_max", "history_bad", "pixels_off_by_more_than_1",
+                                     "bit_exact_hit")})
+    assert rep["identity_bad"] == 0, (tag, rep)
+    assert rep["t_bad"] == 0 and rep["n_bad"] == 0 and rep["material_bad"] == 0, (tag, rep)
+    assert rep["linear_bad"] <= rep["rays"] // 100000, (tag, rep)
+    assert rep["history_bad"] <= rep["rays"] // 100000, (tag, rep)
+    return rep
+
+
+@pytest.fixture(scope="module")
+def bench_views(cuda):
+    from stratum_hyperdetail_b200.batch import Batch
+    from stratum_hyperdetail_b200.views import View
+    views = []
+    for p in POSES.values():
+        v = View(WIDTH, HEIGHT)
+        v.set_pose(SEED, p["origin"], p["pos"], p["yaw"], p["pitch"])
+        views.append(v)
+    b = Batch(views)
+    torch.cuda.synchronize()
+    yield views, b
+    b.graph = None
+    del b, views
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.parametrize("k", SAMPLES)
+def test_bench_poses_full_frames(cuda, oracle, bench_views, k):
+    sb = cuda
+    views, b = bench_views
+    P = WIDTH * HEIGHT
+    n = len(views)
+    hist = [seeded_history(P, k, 1000 * k + i) for i in range(n)]
+    # the drop-in path, view by view
+    arm(views, hist, [k] * n)
+    plain = []
+    for v in views:
+        drop_in(v, sb)
+        plain.append(grab(v))
+    # the batched path: every view in one launch per kernel
+    arm(views, hist, [k] * n)
+    b.render()
+    batched = [grab(v) for v in views]
+    # the captured frame: stepViews takes sample k-1 to k, then refresh, build and render
+    if b.graph is None:
+        arm(views, hist, [k - 1] * n)
+        b.frame()  # one eager frame initialises every lazily sized launch before capture
+        b.capture()
+    arm(views, hist, [k - 1] * n)
+    b.replay()
+    graph = [grab(v) for v in views]
+    torch.cuda.synchronize()
+    for v in views:
+        assert v.C[19].item() == float(k)
+
+    for i, (name, p) in enumerate(POSES.items()):
+        o = ol.setup_pose(oracle, SEED, p["pos"], p["yaw"], p["pitch"], WIDTH, HEIGHT, sample=k, origin=p["origin"])
+        second = np.zeros(P, np.float32)
+        want = ol.render(oracle, o, WIDTH, HEIGHT, second=second, history=hist[i].copy())
+        got = host(plain[i])
+        check_against_oracle(f"{name} sample {k} drop-in", got, want, second)
+        assert same_bits(host(batched[i]), got), f"{name} sample {k}: batched != drop-in"
+        assert same_bits(host(graph[i]), got), f"{name} sample {k}: graph replay != drop-in"
+        rep = fp64_report(oracle, o, got, WIDTH, HEIGHT)
+        print(f"{name} sample {k} fp64", rep)
+        check_fp64(rep)
+
+
+def test_random_views_against_oracle(cuda, oracle):
+    """Eight views of the multi-view workload, batched in one launch and through
+    the drop-in strips, each at its own sample count."""
+    from stratum_hyperdetail_b200.batch import Batch
+    from stratum_hyperdetail_b200.views import View
+    sb = cuda
+    specs = random_view_specs(8)
+    views, hist = [], []
+    for i, (k, w, h, seed, origin, pos, yaw, pitch) in enumerate(specs):
+        v = View(w, h)
+        v.set_pose(seed, origin, pos, yaw, pitch)
+        views.append(v)
+        hist.append(seeded_history(w * h, k, 77 + i))
+    samples = [spec[0] for spec in specs]
+    b = Batch(views)
+    arm(views, hist, samples)
+    b.render()
+    batched = [grab(v) for v in views]
+    arm(views, hist, samples)
+    plain = []
+    for v in views:
+        drop_in(v, sb)
+        plain.append(grab(v))
+    torch.cuda.synchronize()
+    for i, (k, w, h, seed, origin, pos, yaw, pitch) in enumerate(specs):
+        o = ol.setup_pose(oracle, seed, pos, yaw, pitch, w, h, sample=k, origin=origin)
+        second = np.zeros(w * h, np.float32)
+        want = ol.render(oracle, o, w, h, second=second, history=hist[i].copy())
+        got = host(batched[i])
+        check_against_oracle(f"view {i} ({w}x{h}, seed {seed}, sample {k}) batched", got, want, second)
+        assert same_bits(host(plain[i]), got), f"view {i}: drop-in != batched"
+        rep = fp64_report(oracle, o, got, w, h)
+        print(f"view {i} fp64", rep)
+        check_fp64(rep)

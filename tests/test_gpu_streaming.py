@@ -1,14 +1,19 @@
-"""Streaming world on the GPU: a camera flies at 40 m altitude and 40 m/s
-across the 64-bit carry of the x lot address (start xl = 0xFFFFFFF0), one
-stepCamera + lot refresh + hierarchy refresh per 60 Hz frame.
+"""Streaming world on the GPU: a camera flies 10 km at 40 m altitude and
+40 m/s (15,000 frames at 60 Hz) across the 64-bit carry of the x lot address
+(start xl = 0xFFFFFFF0), one stepCamera + lot refresh + hierarchy refresh per
+frame.
 
-Checks, at the carry crossing and after it:
+Checks:
   * every cell crossing refreshes exactly one 128-lot column, other frames none;
-  * the incrementally maintained table (World, Tags, Nodes) equals a table
-    built from scratch by the CPU oracle for the same origin, bit for bit;
-  * 65,536 uniformly random rays agree hierarchy-vs-exhaustive on the GPU
-    (distance bit for bit, identity except exact ties), and a subset agrees
-    with the oracle's hierarchy query bit for bit.
+  * at the carry and at checkpoints along the flight, the incrementally
+    maintained table (World, Tags, Nodes) equals a table built from scratch by
+    the CPU oracle for the same origin, bit for bit;
+  * at every 12th cell crossing and around the carry, 65,536 uniformly random
+    rays agree hierarchy-vs-exhaustive on the GPU: distance bit for bit on
+    every ray, and where the two name different features, both features are
+    re-tested on the ray (GPU and oracle) and must give that distance bit for
+    bit -- an exact tie, not a disagreement; a subset agrees with the oracle's
+    hierarchy query bit for bit.
 """
 import math
 
@@ -39,8 +44,14 @@ def trace_rays(v, rays, exhaustive):
     return out.cpu().numpy().reshape(-1, 8)
 
 
+FRAMES = 15000          # 10 km at 40 m/s, 60 Hz
+CARRY_FRAME = 837       # xl 0xFFFFFFFF -> 0, xh 0 -> 1
+TABLE_CHECKS = {500, 836, 837, 1000, 7500, 15000}
+
+
 def test_flight_across_the_carry(cuda, oracle):
     import stratum_hyperdetail_b200 as sb
+    import stratum_hyperdetail_b200.rays as sr
     from stratum_hyperdetail_b200.views import View
     s = torch.cuda.current_stream().cuda_stream
     v = View(256, 144)
@@ -49,8 +60,8 @@ def test_flight_across_the_carry(cuda, oracle):
     v.I[0] = 1.0    # forward
     rng = np.random.default_rng(1)
     prev = v.Origin.cpu().numpy().view(np.uint32).copy()
-    checked, crossings = [], 0
-    for frame in range(1, 1001):
+    checked, crossings, ties = [], 0, 0
+    for frame in range(1, FRAMES + 1):
         sb.call("stratum_stepCamera", sb.ptr(v.C), sb.ptr(v.Origin), sb.ptr(v.I), 1.0 / 60.0, 256, 144, s)
         v.refresh()
         org = v.Origin.cpu().numpy().view(np.uint32).copy()
@@ -63,7 +74,8 @@ def test_flight_across_the_carry(cuda, oracle):
             assert org[0] == 0 and prev[0] == 0xFFFFFFFF and org[1] == prev[1] + 1, (frame, prev, org)
         crossings += moved
         prev = org
-        if frame in (500, 836, 837, 1000):
+        rays_check = frame in (CARRY_FRAME - 1, CARRY_FRAME) or (moved and crossings % 12 == 0)
+        if frame in TABLE_CHECKS or rays_check:
             torch.cuda.synchronize()
             C = v.C.cpu().numpy()
             # incremental GPU table == from-scratch CPU table for this origin
@@ -73,23 +85,37 @@ def test_flight_across_the_carry(cuda, oracle):
             oracle.f("clearQueue")(ref.Queue)
             oracle.f("prepareLots")(ref.Origin, ref.C, ref.World, ref.Tags, ref.Queue)
             oracle.build_bounds(ref.Queue, ref.World, ref.Nodes)
-            assert np.array_equal(v.World.cpu().numpy().view(np.uint32), ref.World.view(np.uint32))
-            assert np.array_equal(v.Tags.cpu().numpy().view(np.uint32), ref.Tags)
-            assert np.array_equal(v.Nodes.cpu().numpy(), ref.Nodes)
+            assert np.array_equal(v.World.cpu().numpy().view(np.uint32), ref.World.view(np.uint32)), frame
+            assert np.array_equal(v.Tags.cpu().numpy().view(np.uint32), ref.Tags), frame
+            assert np.array_equal(v.Nodes.cpu().numpy(), ref.Nodes), frame
+            if not rays_check:
+                continue
             # hierarchy vs exhaustive over 65,536 random rays
             rays = random_rays(rng, RAYS)
             h, e = trace_rays(v, rays, False), trace_rays(v, rays, True)
             same_t = h[:, 0].view(np.uint32) == e[:, 0].view(np.uint32)
             assert same_t.all(), np.where(~same_t)[0][:10]
-            diff_id = h[:, 1] != e[:, 1]
-            # an identity may differ only where two features tie exactly (same distance)
-            assert diff_id.sum() <= RAYS // 10000, diff_id.sum()
+            # an identity may differ only where two features tie exactly: re-test both on the ray
+            R = torch.from_numpy(rays).cuda()
+            rep = sr.compare_hierarchy(v, R, torch.from_numpy(h).cuda(), torch.from_numpy(e).cuda())
+            assert rep["distance_mismatches"] == 0 and rep["identity_mismatches_non_tie"] == 0, (frame, rep)
+            diff = np.flatnonzero((h[:, 1] != e[:, 1]) | (h[:, 7] != e[:, 7]))
+            if len(diff):
+                for res in (h, e):
+                    ids = np.stack([res[diff, 7], res[diff, 1]], 1).astype(np.int32)
+                    g = sr.retest(v, R[torch.from_numpy(diff).cuda()], torch.from_numpy(ids).cuda()).cpu().numpy()
+                    o = oracle.retest_features(ref.World, ref.Origin, rays[diff], ids)
+                    feat = res[diff, 1] >= 0
+                    assert np.array_equal(g[feat].view(np.uint32), o[feat].view(np.uint32)), frame
+                    assert np.array_equal(g[feat, 0].view(np.uint32), h[diff[feat], 0].view(np.uint32)), frame
+            ties += rep["identity_ties"]
             sub = rays[:2048]
             o = oracle.trace_rays(ref.World, ref.Nodes, ref.Origin, sub, False)
             assert np.array_equal(h[:2048].view(np.uint32), o.view(np.uint32))
             checked.append((frame, int(org[0]), int(org[1]), int((h[:, 1] >= 0).sum())))
     # the carry was crossed: xl wrapped past 0 and xh went from 0 to 1
-    # 1000 frames x 0.67 m = 667 m = 19 cells: xl 0xFFFFFFF0 -> 3 with xh 0 -> 1 (carry at frame 837)
-    assert crossings == 19 and checked[-1][1:3] == (3, 1), (crossings, checked)
+    # 15,000 frames x 0.67 m = 10 km = 278 cells: xl 0xFFFFFFF0 -> 0x106 with xh 0 -> 1 (carry at frame 837)
+    assert crossings == 278 and tuple(prev[:2]) == (0x106, 1), (crossings, prev)
     assert any(c[1:3] == (0xFFFFFFFF, 0) for c in checked) and any(c[1:3] == (0, 1) for c in checked), checked
-    print("streaming checkpoints (frame, xl, xh, hits of 65,536):", checked)
+    assert len(checked) >= 24, checked
+    print("streaming checkpoints (frame, xl, xh, hits of 65,536):", checked, "exact ties:", ties)
