@@ -221,7 +221,9 @@ int stratum_autotune(stratum_view* views, int n, void* scratch, unsigned long lo
  * Limits: at most STRATUM_NOALLOC_MAX_VIEWS views per call; more returns
  * STRATUM_ELIMIT and launches nothing.  The first call on each device looks up
  * the array's address (cudaGetSymbolAddress); make that first call before any
- * stream capture on that device.  All calls share the one array: calls whose
+ * stream capture on that device.  The address is kept per device context: after
+ * a cudaDeviceReset the next call looks it up again, so make that call, too,
+ * outside a capture.  All calls share the one array: calls whose
  * work overlaps on the GPU (unordered streams) race and corrupt each other's
  * frames, so order them on one stream or with events.  Each call clears the
  * queue counters and rewrites the per-view constants before using them. */

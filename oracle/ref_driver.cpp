@@ -158,6 +158,32 @@ void ref_resolveRows(const float* Linear, float* History, unsigned* Pixels, cons
       resolveFrame(Linear, History, Pixels, C, Hit, Surface, width, height);
     }
 }
+// trace, shade and resolve of the listed rows only (timing samples spread over
+// a frame): each pass runs every pixel of those rows, in parallel over pixels;
+// a row is the reference's strip of one row (rowStart = y, rowCount = 1).
+void ref_renderRows(const float* World, const float* Nodes, const unsigned* Origin, const float* C, float* Hit,
+                    float* Surface, float* Linear, float* History, unsigned* Pixels, int width, int height,
+                    const int* rows, int nrows, int nthreads) {
+  const long n = long(nrows) * width;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads(nthreads))
+  for (long i = 0; i < n; i++) {
+    const int y = rows[i / width], x = int(i % width);
+    set_pixel(x, 0);
+    tracePrimary(World, Nodes, Origin, C, Hit, Surface, width, height, y, 1);
+  }
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads(nthreads))
+  for (long i = 0; i < n; i++) {
+    const int y = rows[i / width], x = int(i % width);
+    set_pixel(x, 0);
+    shadePixels(World, Origin, C, Hit, Surface, Linear, width, height, y, 1);
+  }
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads(nthreads))
+  for (long i = 0; i < n; i++) {
+    const int y = rows[i / width], x = int(i % width);
+    set_pixel(x, y);
+    resolveFrame(Linear, History, Pixels, C, Hit, Surface, width, height);
+  }
+}
 void ref_probeGrammar(const float* Inputs, float* Output) { one_thread(); probeGrammar(Inputs, Output); }
 
 // Feature records of one group: 10 floats each [p.xyz, h.xyz, shape, material,

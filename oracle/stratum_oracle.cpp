@@ -1569,6 +1569,18 @@ void orc_traceRays(const float* W, const float* N, const uint32_t* O, const floa
     traceRayOrc(W, N, O, mk(q[0], q[1], q[2]), mk(q[3], q[4], q[5]), q[6], exhaustive != 0, out + size_t(i) * 8);
   }
 }
+// trace, shade and resolve of the listed rows only, in parallel over pixels.
+void orc_renderRows(const float* W, const float* N, const uint32_t* O, const float* C, float* Hit, float* Surf,
+                    float* Lin, float* Hist, uint32_t* Px, int width, int height, const int32_t* rows, int nrows,
+                    int nthreads) {
+  const long n = long(nrows) * width;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(useThreads(nthreads))
+  for (long i = 0; i < n; i++) tracePixel(W, N, O, C, Hit, Surf, width, height, int(i % width), rows[i / width], nullptr, nullptr);
+#pragma omp parallel for schedule(dynamic, 64) num_threads(useThreads(nthreads))
+  for (long i = 0; i < n; i++) shadePixel(W, O, C, Hit, Surf, Lin, width, height, int(i % width), rows[i / width], nullptr);
+#pragma omp parallel for schedule(dynamic, 64) num_threads(useThreads(nthreads))
+  for (long i = 0; i < n; i++) resolvePixel(Lin, Hist, Px, C, Hit, Surf, width, height, int(i % width), rows[i / width]);
+}
 // One named (slot, fid) feature per ray, intersected in its lot frame as the
 // trace forms it (world.cu:37-56, sink.cu:21, geometry.cu:33-114).
 void orc_retestFeatures(const float* W, const uint32_t* O, const float* rays, const int32_t* ids, int n, float* out,

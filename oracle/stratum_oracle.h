@@ -77,6 +77,10 @@ void orc_traceRays(const float* World, const float* Nodes, const uint32_t* Origi
 void orc_resolveRows(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
                      const float* Surface, int width, int height, int rowStart, int rowCount, int nthreads);
 void orc_probeGrammar(const float* Inputs, float* Output);
+/* trace + shade + resolve of the listed rows (rows[nrows]) only. */
+void orc_renderRows(const float* World, const float* Nodes, const uint32_t* Origin, const float* C, float* Hit,
+                    float* Surface, float* Linear, float* History, uint32_t* Pixels, int width, int height,
+                    const int32_t* rows, int nrows, int nthreads);
 /* rays n x 7 as orc_traceRays; ids n x 2 [slot, fid]; out n x 4 [t, n.xyz] of
  * that one feature on that ray (t = 2000 if missed). */
 void orc_retestFeatures(const float* World, const uint32_t* Origin, const float* rays, const int32_t* ids, int n,

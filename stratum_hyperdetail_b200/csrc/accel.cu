@@ -4,6 +4,8 @@
 // writes the 64 leaves of each queued lot, reduceGroupBounds one level.  The
 // B200 form, buildBVH, refreshes every queued lot in one launch with one block
 // per lot (hierarchy.cuh); it produces the same bits.
+#include <mutex>
+
 #include "common_api.cuh"
 #include "hierarchy.cuh"
 
@@ -44,17 +46,22 @@ __global__ void __launch_bounds__(64) buildLotHierarchyK(const uint32_t* Q, cons
 
 using namespace st;
 
-// Resident blocks of the hierarchy kernel on this device (SMs x occupancy).
+// Resident blocks of the hierarchy kernel on the current device (SMs x
+// occupancy), computed once per device; std::call_once publishes it to
+// concurrent first callers.
 int stratumHierarchyGrid() {
-  static int blocks = 0;
-  if (!blocks) {
-    int dev = 0, sms = 148, per = 0;
-    cudaGetDevice(&dev);
+  constexpr int kDevices = 64;
+  static std::once_flag once[kDevices];
+  static int blocks[kDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) dev = 0;
+  std::call_once(once[dev], [dev] {
+    int sms = 148, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, buildLotHierarchyK, 64, 0);
-    blocks = sms * (per > 0 ? per : 8);
-  }
-  return blocks;
+    blocks[dev] = sms * (per > 0 ? per : 8);
+  });
+  return blocks[dev];
 }
 
 extern "C" {

@@ -28,6 +28,8 @@
 //
 // The tile queues reset themselves: the last warp to find a queue empty zeroes
 // its counters, so consecutive launches (and graph replays) need no memset.
+#include <mutex>
+
 #include "batch.cuh"
 #include "common_api.cuh"
 #include "hierarchy.cuh"
@@ -315,19 +317,34 @@ constexpr size_t traceSmem(int threads) { return size_t(threads / 32) * sizeof(W
 
 enum Parts { kTrace = 1, kShade = 2 };
 
+// Persistent grids of one block size on one device: the resident-block count of
+// each kernel, computed once per (block size, device) and published through
+// std::call_once, so concurrent first calls (the render server's scheduler and
+// a direct caller) all see the four grids complete.
+constexpr int kGridDevices = 64;
+struct PersistentGrids { int trace, shade, light, resolve; };
+
 template <int T>
 int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratch* S, cudaStream_t s, int parts) {
-  static int traceGrid = 0, shadeGrid = 0, resolveGrid = 0, lightGrid = 0;
-  if (!traceGrid) {
-    traceGrid = residentBlocks(traceViewsK<T>, T, traceSmem(T));
-    shadeGrid = residentBlocks(shadeViewsK<T>, T);
-    resolveGrid = residentBlocks(resolveViewsK<T>, T);
-    lightGrid = residentBlocks(lightViewsK<T>, T);
-  }
-  if (parts & kTrace) traceViewsK<T><<<traceGrid, T, traceSmem(T), s>>>(V, n, t.grab, t.order, S);
-  if (parts & kShade) shadeViewsK<T><<<shadeGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
-  if (parts & kShade) lightViewsK<T><<<lightGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
-  if (parts & kShade) resolveViewsK<T><<<resolveGrid, T, 0, s>>>(V, n, t.grab, t.order, S);
+  static std::once_flag once[kGridDevices];
+  static PersistentGrids grids[kGridDevices];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return -int(e);
+  if (dev < 0 || dev >= kGridDevices) return STRATUM_EINVAL;
+  std::call_once(once[dev], [&] {
+    PersistentGrids g;
+    g.trace = residentBlocks(traceViewsK<T>, T, traceSmem(T));
+    g.shade = residentBlocks(shadeViewsK<T>, T);
+    g.light = residentBlocks(lightViewsK<T>, T);
+    g.resolve = residentBlocks(resolveViewsK<T>, T);
+    grids[dev] = g;
+  });
+  const PersistentGrids& g = grids[dev];
+  if (parts & kTrace) traceViewsK<T><<<g.trace, T, traceSmem(T), s>>>(V, n, t.grab, t.order, S);
+  if (parts & kShade) shadeViewsK<T><<<g.shade, T, 0, s>>>(V, n, t.grab, t.order, S);
+  if (parts & kShade) lightViewsK<T><<<g.light, T, 0, s>>>(V, n, t.grab, t.order, S);
+  if (parts & kShade) resolveViewsK<T><<<g.resolve, T, 0, s>>>(V, n, t.grab, t.order, S);
   return launchStatus();
 }
 
@@ -363,15 +380,46 @@ static __device__ __align__(256) unsigned char gNoAllocScratch[kNoAllocBytes];
 
 }  // namespace st
 
+#include <cuda.h>
 #include <mutex>
 
 namespace {
-// Device address of gNoAllocScratch per device ordinal, looked up on the first
-// call made with that device current.  Host code must not use the array's name
-// as an address: on the host it is only a stand-in for the device symbol.
+// Device address of gNoAllocScratch per device ordinal, looked up with that
+// device current on the first call in each of its contexts.  Host code must
+// not use the array's name as an address: on the host it is only a stand-in
+// for the device symbol.  The address belongs to the context the module was
+// loaded into, so it is cached with that context's unique id: after a
+// cudaDeviceReset the next call finds a new context and looks it up again.
 constexpr int kMaxDevices = 128;
 std::mutex gNoAllocLock;
-void* gNoAllocAddr[kMaxDevices] = {};
+struct NoAllocSlot { unsigned long long ctx; void* addr; };
+NoAllocSlot gNoAllocAddr[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique id of the calling thread's current context (0 if none or unknown),
+// through the driver entry points the runtime hands out.
+unsigned long long currentContextId() {
+  static std::once_flag once;
+  static CtxGetCurrentFn getCurrent = nullptr;
+  static CtxGetIdFn getId = nullptr;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      getCurrent = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      getId = reinterpret_cast<CtxGetIdFn>(f);
+  });
+  CUcontext ctx = nullptr;
+  unsigned long long id = 0;
+  if (!getCurrent || !getId || getCurrent(&ctx) != CUDA_SUCCESS || !ctx || getId(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 int noAllocScratch(void** out) {
   int dev = 0;
@@ -379,13 +427,16 @@ int noAllocScratch(void** out) {
   if (e != cudaSuccess) return -int(e);
   if (dev < 0 || dev >= kMaxDevices) return STRATUM_EINVAL;
   std::lock_guard<std::mutex> hold(gNoAllocLock);
-  if (!gNoAllocAddr[dev]) {
+  NoAllocSlot& slot = gNoAllocAddr[dev];
+  const unsigned long long ctx = currentContextId();
+  if (!slot.addr || ctx == 0 || slot.ctx != ctx) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, st::gNoAllocScratch);
     if (e != cudaSuccess || !p) return e != cudaSuccess ? -int(e) : STRATUM_EINVAL;
-    gNoAllocAddr[dev] = p;
+    slot.addr = p;
+    slot.ctx = currentContextId();  // the lookup has made the device's context current
   }
-  *out = gNoAllocAddr[dev];
+  *out = slot.addr;
   return STRATUM_OK;
 }
 }  // namespace

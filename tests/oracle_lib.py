@@ -73,12 +73,22 @@ class _Lib:
         self.hashfn = getattr(L, p + ("hashU"))
         self.hashfn.restype = ct.c_uint32
         self.hashfn.argtypes = [ct.c_uint32]
+        rr = getattr(L, p + "renderRows")
+        rr.restype = None
+        rr.argtypes = [f32p, f32p, u32p, f32p, f32p, f32p, f32p, f32p, u32p, ct.c_int, ct.c_int, i32p, ct.c_int,
+                       ct.c_int]
         self.taghash = getattr(L, p + "tag_hash")
         self.taghash.restype = ct.c_uint32
         self.taghash.argtypes = [u32p, ct.c_int]
 
     def f(self, name):
         return getattr(self.lib, self.prefix + name)
+
+    def render_rows(self, s, bufs, width, height, rows, nthreads=0):
+        """trace + shade + resolve of the listed rows of a frame (timing samples)."""
+        hit, surf, lin, hist, px = bufs
+        self.f("renderRows")(s.World, s.Nodes, s.Origin, s.C, hit, surf, lin, hist, px, int(width), int(height),
+                             np.ascontiguousarray(rows, np.int32), len(rows), nthreads)
 
     # -- world -------------------------------------------------------------
     def offset_tag(self, origin, dx, dz):
