@@ -98,7 +98,10 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rows", type=int, default=48, help="rows per pose in a CPU sample (spread over the frame)")
     ap.add_argument("--poses", default=",".join(POSES), help="comma-separated subset of the six poses (profiling)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="length of each serving run (0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
+                    help="length of the 256-session serving runs (the serving workload; 0: skip serving)")
+    ap.add_argument("--serve-seconds-short", type=float, default=10.0,
+                    help="length of the 64-session serving runs")
     ap.add_argument("--serve-views", type=int, default=8, help="views per serving batch")
     ap.add_argument("--tune", default=None, help="threads,grab,order of the batched trace (default: autotune)")
     ap.add_argument("--random-views", type=int, default=64, help="views of the random multi-view scenario (0: skip)")
@@ -764,11 +767,11 @@ def ours_arm(args):
         serving = {
             "mixed_256_sessions": serve_poisson(200.0, 256, args.serve_seconds, (768, 1024, 1600, 1920), 150 << 30,
                                                 args.serve_views, 3, tune_t),
-            "sessions_64_at_1600x900": serve_poisson(200.0, 64, args.serve_seconds, (1600,), 150 << 30,
+            "sessions_64_at_1600x900": serve_poisson(200.0, 64, args.serve_seconds_short, (1600,), 150 << 30,
                                                      args.serve_views, 3, tune_t, seed=2),
             # twice the offered load (580 M rays/s): headroom of the same 64 sessions
-            "sessions_64_at_1600x900_400rps": serve_poisson(400.0, 64, args.serve_seconds, (1600,), 150 << 30,
-                                                            args.serve_views, 3, tune_t, seed=4),
+            "sessions_64_at_1600x900_400rps": serve_poisson(400.0, 64, args.serve_seconds_short, (1600,),
+                                                            150 << 30, args.serve_views, 3, tune_t, seed=4),
             # a budget that holds about two thirds of the sessions: LRU eviction and exact resumption at work
             "mixed_256_sessions_40gb_budget": serve_poisson(200.0, 256, args.serve_seconds, (768, 1024, 1600, 1920),
                                                             40 << 30, args.serve_views, 3, tune_t, seed=3),

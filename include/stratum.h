@@ -296,7 +296,10 @@ int stratum_server_submit(stratum_server* server, int session, const stratum_pos
 int stratum_server_wait(stratum_server* server, long long request, int timeout_ms, stratum_request_info* info);
 int stratum_server_stats_get(stratum_server* server, stratum_server_stats* stats);
 /* Host-side fault injection for tests: kind 1 = the next `count` session
- * admissions fail as if the device allocation had failed. */
+ * admissions fail as if the device allocation had failed; kind 2 = the next
+ * `count` batch launches fail after refreshViews, with part of the batch's work
+ * already queued (its requests fail once that work has drained; its sessions
+ * restart their sampling on their next request). */
 int stratum_server_inject(stratum_server* server, int kind, int count);
 /* The last frame (RGBA8) and accumulation buffer of a resident session, copied
  * to host memory (test and tooling; synchronises the session). */

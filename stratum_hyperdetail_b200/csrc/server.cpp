@@ -10,12 +10,16 @@
 // Admission is by an HBM budget: a session is admitted when its bytes fit;
 // otherwise least recently used sessions that are idle (nothing queued in a
 // launched batch) are evicted.  Eviction snapshots what the future needs (camera
-// state, table origin, accumulation buffer) to pinned host memory and frees the
-// device memory; re-admission restores the snapshot and rebuilds the table and
-// hierarchy from the seed, so the session continues exactly as if it had never
-// left (the world is a pure function of seed and address).  Eviction and
-// admission are ordered on one admission stream that batches wait for with an
-// event: the scheduler thread never waits on the device for them.
+// state, table origin, accumulation buffer) to pinned host memory (pinned when
+// the session is opened, not while the scheduler holds its lock) and frees the
+// device memory to the server's own memory pool, which keeps it mapped for the
+// next admission; re-admission clears only what must start at zero (camera,
+// input, table, tags; History when there is no snapshot), restores the
+// snapshot and rebuilds the table and hierarchy from the seed, so the session
+// continues exactly as if it had never left (the world is a pure function of
+// seed and address).  Eviction and admission are ordered on one admission
+// stream that batches wait for with an event: the scheduler thread never waits
+// on the device for them.
 //
 // The scheduler thread keeps `streams` batch slots.  Whenever a slot is free it
 // takes the oldest pending request of every idle session (up to `max_views`),
@@ -24,6 +28,13 @@
 // the RGBA8 read-back -- on that slot's stream.  Requests arriving while
 // batches run join the next free slot, so their work overlaps on the device.
 // A request of k samples rides in k consecutive batches.
+//
+// A batch whose launch fails after part of its work was queued keeps its slot
+// (and its sessions) busy until that work has drained from the slot's stream;
+// only then are its requests failed and its sessions released, so no pinned
+// staging buffer is rewritten and no session memory is freed under queued
+// work.  Sessions of a failed batch restart their sampling on their next
+// request (their camera state may have been stepped).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -83,7 +94,7 @@ struct Session {
   int id, seed, width, height;
   Layout lay;
   char* base = nullptr;
-  bool resident = false, inflight = false, started = false;
+  bool resident = false, inflight = false, started = false, restart = false;
   std::deque<Request*> queue;
   stratum_pose last{};
   double lastUse = 0.0;
@@ -118,6 +129,7 @@ struct Slot {
   int* hFlags = nullptr;
   std::vector<Request*> reqs;
   bool busy = false;
+  int failStatus = STRATUM_OK;  // a batch that failed after enqueueing: its requests fail on completion
 };
 
 bool samePose(const stratum_pose& a, const stratum_pose& b) { return std::memcmp(&a, &b, sizeof a) == 0; }
@@ -136,6 +148,7 @@ struct stratum_server {
   std::atomic<bool> stop{false};
   cudaStream_t admitStream = nullptr;
   cudaEvent_t admitDone = nullptr;  // recorded after each admission's device work
+  cudaMemPool_t pool = nullptr;     // session memory; keeps freed blocks mapped up to the budget
   std::unordered_map<int, std::unique_ptr<Session>> sessions;
   int nextSession = 1;
   std::unordered_map<long long, std::unique_ptr<Request>> requests;
@@ -146,6 +159,7 @@ struct stratum_server {
   std::vector<double> latencies;
   double rays = 0.0, firstSubmit = -1.0, lastDone = -1.0;
   int injectAllocFail = 0;
+  int injectLaunchFail = 0;  // fail launches after refreshViews (work already queued)
 };
 
 namespace {
@@ -168,10 +182,7 @@ void finish(stratum_server* S, Request* r, int status) {
 // Only idle sessions are evicted: their last batch has completed.
 int evict(stratum_server* S, Session& s) {
   size_t P = size_t(s.width) * size_t(s.height);
-  if (!s.snap && cudaMallocHost(reinterpret_cast<void**>(&s.snap), P * 16 + 512) != cudaSuccess) {
-    s.snap = nullptr;
-    return -int(cudaGetLastError());
-  }
+  if (!s.snap) return STRATUM_EINVAL;  // pinned at open
   cudaError_t e = cudaMemcpyAsync(s.snap + P * 16, s.at<float>(s.lay.C), 64 * 4, cudaMemcpyDeviceToHost, S->admitStream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.snap + P * 16 + 256, s.at<unsigned>(s.lay.Origin), 16, cudaMemcpyDeviceToHost, S->admitStream);
@@ -208,10 +219,16 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
     return -int(cudaErrorMemoryAllocation);
   }
   void* p = nullptr;
-  cudaError_t e = cudaMallocAsync(&p, need, S->admitStream);
+  cudaError_t e = cudaMallocFromPoolAsync(&p, need, S->pool, S->admitStream);
   if (e != cudaSuccess) return -int(e);
   s.base = static_cast<char*>(p);
-  e = cudaMemsetAsync(s.base, 0, need, S->admitStream);
+  // Only what is read before it is written starts at zero: camera, origin and
+  // input, the table and its tags (every lot is then described and its
+  // hierarchy built), and History unless a snapshot restores it.  Nodes, the
+  // frame buffers and the group cache's entries are written before any read.
+  e = cudaMemsetAsync(s.base, 0, s.lay.Nodes, S->admitStream);
+  if (e == cudaSuccess && !s.hasSnap)
+    e = cudaMemsetAsync(s.base + s.lay.History, 0, size_t(s.width) * s.height * 16, S->admitStream);
   int st = e == cudaSuccess ? STRATUM_OK : -int(e);
   if (st == STRATUM_OK)
     st = stratum_initCamera(s.at<float>(s.lay.C), s.at<unsigned>(s.lay.Origin), s.seed,
@@ -226,10 +243,6 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
       e = cudaMemcpyAsync(s.at<unsigned>(s.lay.Origin), s.snap + P * 16 + 256, 16, cudaMemcpyHostToDevice, S->admitStream);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(s.at<float>(s.lay.History), s.snap, P * 16, cudaMemcpyHostToDevice, S->admitStream);
-    if (e != cudaSuccess) st = -int(e);
-  }
-  if (st == STRATUM_OK && !s.pinnedOut) {
-    e = cudaMallocHost(reinterpret_cast<void**>(&s.pinnedOut), size_t(s.width) * s.height * 4);
     if (e != cudaSuccess) st = -int(e);
   }
   if (st == STRATUM_OK) {  // batches wait for this event on their own streams; the host does not
@@ -248,6 +261,9 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
   return STRATUM_OK;
 }
 
+int enqueue(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs, int n);
+void deferFailure(Slot& sl, const std::vector<Request*>& reqs, int status);
+
 int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
   const int n = int(reqs.size());
   const double t = nowMs();
@@ -259,7 +275,8 @@ int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
     int flags = 0;
     if (!r->poseApplied) {  // first sample of this request: place the camera
       flags |= 1;
-      if (!s.started || !samePose(s.last, r->pose)) flags |= 2;
+      if (!s.started || s.restart || !samePose(s.last, r->pose)) flags |= 2;
+      s.restart = false;
       s.last = r->pose;
       s.started = true;
       r->poseApplied = true;
@@ -268,10 +285,31 @@ int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
     if (r->tStart < 0) r->tStart = t;
   }
   cudaStream_t st = sl.stream;
-  stratum_stream_t ss = reinterpret_cast<stratum_stream_t>(st);
   // sessions admitted for this batch: their allocation, initialisation and
   // restored snapshot are ordered on the admission stream
   cudaError_t e = cudaStreamWaitEvent(st, S->admitDone, 0);
+  if (e != cudaSuccess) return -int(e);  // nothing queued yet
+  int s = enqueue(S, sl, reqs, n);
+  if (s != STRATUM_OK) {
+    deferFailure(sl, reqs, s);
+    return STRATUM_OK;  // the requests fail when the queued work has drained
+  }
+  e = cudaEventRecord(sl.done, st);
+  if (e != cudaSuccess) {
+    deferFailure(sl, reqs, -int(e));
+    return STRATUM_OK;
+  }
+  sl.reqs = reqs;
+  sl.busy = true;
+  S->batches++;
+  return STRATUM_OK;
+}
+
+// The device work of one batch on its slot's stream.
+int enqueue(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs, int n) {
+  cudaStream_t st = sl.stream;
+  stratum_stream_t ss = reinterpret_cast<stratum_stream_t>(st);
+  cudaError_t e = cudaSuccess;
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.dViews, sl.hViews, sizeof(stratum_view) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.dPoses, sl.hPoses, sizeof(stratum_pose) * n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(sl.dFlags, sl.hFlags, sizeof(int) * n, cudaMemcpyHostToDevice, st);
@@ -280,6 +318,10 @@ int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
   if ((s = stratum_applyPoses(sl.dViews, sl.dPoses, sl.dFlags, n, ss)) != STRATUM_OK) return s;
   if ((s = stratum_stepViews(sl.dViews, n, ss)) != STRATUM_OK) return s;
   if ((s = stratum_refreshViews(sl.dViews, n, ss)) != STRATUM_OK) return s;
+  if (S->injectLaunchFail > 0) {  // host-side fault injection: work is already queued on the stream
+    S->injectLaunchFail--;
+    return -int(cudaErrorLaunchFailure);
+  }
   if ((s = stratum_buildViews(sl.dViews, n, ss)) != STRATUM_OK) return s;
   if ((s = stratum_renderViews(sl.dViews, n, sl.scratch, sl.scratchBytes, &S->tune, ss)) != STRATUM_OK) return s;
   for (int i = 0; i < n; i++) {
@@ -290,15 +332,37 @@ int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
                         cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return -int(e);
   }
-  e = cudaEventRecord(sl.done, st);
-  if (e != cudaSuccess) return -int(e);
-  sl.reqs = reqs;
-  sl.busy = true;
-  S->batches++;
   return STRATUM_OK;
 }
 
+// A batch that failed after part of it was queued: hold the slot until that
+// work drains (an event on the slot's stream, or a synchronize if even the
+// record fails), then fail its requests in complete().
+void deferFailure(Slot& sl, const std::vector<Request*>& reqs, int status) {
+  sl.reqs = reqs;
+  sl.failStatus = status;
+  sl.busy = true;
+  if (cudaEventRecord(sl.done, sl.stream) != cudaSuccess) {
+    cudaStreamSynchronize(sl.stream);
+    cudaEventRecord(sl.done, sl.stream);
+  }
+}
+
 void complete(stratum_server* S, Slot& sl) {
+  if (sl.failStatus != STRATUM_OK) {
+    for (Request* r : sl.reqs) {
+      Session& s = *S->sessions[r->session];
+      s.inflight = false;
+      s.restart = true;
+      s.lastUse = nowMs();
+      s.queue.pop_front();
+      finish(S, r, sl.failStatus);
+    }
+    sl.reqs.clear();
+    sl.failStatus = STRATUM_OK;
+    sl.busy = false;
+    return;
+  }
   for (Request* r : sl.reqs) {
     Session& s = *S->sessions[r->session];
     s.inflight = false;
@@ -355,10 +419,11 @@ void schedule(stratum_server* S) {
       }
       if (reqs.empty()) break;
       int st = launch(S, sl, reqs);
-      if (st != STRATUM_OK) {  // a launch that failed fails its requests; the server keeps serving
+      if (st != STRATUM_OK) {  // nothing was queued: fail its requests now; the server keeps serving
         for (Request* r : reqs) {
           Session& s = *S->sessions[r->session];
           s.inflight = false;
+          s.restart = true;
           s.queue.pop_front();
           finish(S, r, st);
         }
@@ -395,8 +460,24 @@ stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_v
   S->maxViews = max_views;
   if (tune) S->tune = *tune;
   if (cudaStreamCreateWithFlags(&S->admitStream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaEventCreateWithFlags(&S->admitDone, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&S->admitDone, cudaEventDisableTiming) != cudaSuccess) {
+    stratum_server_destroy(S.release());
     return nullptr;
+  }
+  // Session memory comes from the server's own pool, which keeps up to the
+  // budget mapped after a free: an eviction followed by an admission reuses
+  // the pages instead of returning them to the driver and mapping them again.
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = S->device;
+  unsigned long long keep = budget_bytes;  // the attribute is a 64-bit count of bytes
+  if (cudaMemPoolCreate(&S->pool, &props) != cudaSuccess ||
+      cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+    stratum_server_destroy(S.release());
+    return nullptr;
+  }
   S->slots.resize(streams);
   for (Slot& sl : S->slots) {
     sl.scratchBytes = stratum_batchScratchBytes(max_views);
@@ -446,6 +527,7 @@ void stratum_server_destroy(stratum_server* S) {
   }
   if (S->admitDone) cudaEventDestroy(S->admitDone);
   if (S->admitStream) cudaStreamDestroy(S->admitStream);
+  if (S->pool) cudaMemPoolDestroy(S->pool);
   delete S;
 }
 
@@ -459,6 +541,15 @@ int stratum_server_open(stratum_server* S, int seed, int width, int height, int*
   s->width = width;
   s->height = height;
   s->lay = Layout::of(width, height, S->groupEntries);
+  // Host staging is pinned here, not on the scheduler thread: the RGBA8
+  // read-back buffer and the eviction snapshot (History, camera, origin).
+  const size_t P = size_t(width) * size_t(height);
+  if (cudaMallocHost(reinterpret_cast<void**>(&s->pinnedOut), P * 4) != cudaSuccess ||
+      cudaMallocHost(reinterpret_cast<void**>(&s->snap), P * 16 + 512) != cudaSuccess) {
+    cudaError_t e = cudaGetLastError();
+    freeSession(S, *s);
+    return -int(e != cudaSuccess ? e : cudaErrorMemoryAllocation);
+  }
   *session = s->id;
   S->sessions[s->id] = std::move(s);
   return STRATUM_OK;
@@ -543,9 +634,10 @@ int stratum_server_stats_get(stratum_server* S, stratum_server_stats* out) {
 }
 
 int stratum_server_inject(stratum_server* S, int kind, int count) {
-  if (!S || kind != 1 || count < 0) return STRATUM_EINVAL;
+  if (!S || (kind != 1 && kind != 2) || count < 0) return STRATUM_EINVAL;
   std::lock_guard<std::mutex> lk(S->mu);
-  S->injectAllocFail = count;
+  if (kind == 1) S->injectAllocFail = count;
+  else S->injectLaunchFail = count;
   return STRATUM_OK;
 }
 

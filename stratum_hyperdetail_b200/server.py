@@ -126,6 +126,10 @@ class Server:
     def inject_alloc_failures(self, count: int):
         check("stratum_server_inject", self.L.stratum_server_inject(self.h, 1, int(count)))
 
+    def inject_launch_failures(self, count: int):
+        """The next `count` batches fail after refreshViews, with part of their work queued."""
+        check("stratum_server_inject", self.L.stratum_server_inject(self.h, 2, int(count)))
+
     def read(self, sid):
         w, h = self.sizes[sid]
         px = np.zeros(w * h, np.uint32)

@@ -128,3 +128,35 @@ def test_wait_times_out_without_losing_the_request(cuda):
     info = srv.wait(rid, timeout_ms=30000)
     assert info.status == 0 and info.samples_done == 8 and info.latency_ms > 0
     srv.close()
+
+
+def test_failed_launch_with_queued_work_keeps_serving(cuda):
+    """A batch that fails after applyPoses, stepViews and refreshViews were
+    queued: its request fails once that work has drained, a session outside it
+    is untouched (bit for bit), and the failed session restarts its sampling
+    on its next request (the frame of a fresh session at that pose, up to the
+    last bit of the running mean's first step)."""
+    from stratum_hyperdetail_b200.server import Server
+    pa = poses_for(0, 3)
+    pb = poses_for(1, 3, origin=(3, 0, 4, 0))
+    want_b = run_alone(7, 128, 72, pb)
+    fresh_a = run_alone(0x5EED, 160, 90, [pa[2]])[0]
+    srv = Server(8 << 30, max_views=4, streams=2)
+    a, b = srv.open(0x5EED, 160, 90), srv.open(7, 128, 72)
+    assert srv.wait_status(srv.submit(a, pa[0])) == 0
+    assert srv.wait_status(srv.submit(b, pb[0])) == 0
+    srv.inject_launch_failures(1)
+    status = srv.wait_status(srv.submit(a, pa[1]))
+    assert status < 0, status
+    for k in (1, 2):
+        assert srv.wait_status(srv.submit(b, pb[k])) == 0
+        px, hist = srv.read(b)
+        assert np.array_equal(px, want_b[k][0]) and np.array_equal(hist, want_b[k][1]), k
+    assert srv.wait_status(srv.submit(a, pa[2])) == 0
+    px, hist = srv.read(a)
+    assert np.allclose(hist, fresh_a[1], rtol=0, atol=1e-6)
+    d = np.abs(px.view(np.uint8).astype(int) - fresh_a[0].view(np.uint8).astype(int))
+    assert d.max() <= 1
+    st = srv.stats()
+    assert st["failed"] == 1 and st["completed"] == 5, st
+    srv.close()
