@@ -1,30 +1,54 @@
-// tracePrimary drop-in (kernels/trace.cu:29-61 of the reference): one thread
-// per pixel over a strip of rows, 8x8 blocks as the reference launches it.
+// tracePrimary drop-in (kernels/trace.cu:29-61 of the reference): every pixel of
+// a strip of rows, in 8x8 pixel blocks as the reference launches it.
+//
+// A block is two warps, each tracing one 8x4 tile with the warp-cooperative
+// traversal of the batched renderer (traverse_coop.cuh): lanes walk their own
+// rays to the hierarchy leaves, and the warp evaluates one (lot, group) at a
+// time for every lane waiting on it, the group's records built once by the
+// random-access grammar and staged in shared memory.  The drop-in has only the
+// reference's buffers, so there is no group cache.  Each ray still visits its
+// leaves in the reference's order with the same running best, so Hit and
+// Surface equal the per-thread traversal (traverse.cuh) bit for bit; building
+// with STRATUM_DROPIN_PER_LANE selects that per-thread form instead.
 #include "common_api.cuh"
-#include "traverse.cuh"
+#include "traverse_coop.cuh"
 
-// Minimum resident 64-thread blocks per SM the register allocation must allow.
-#ifndef STRATUM_TRACE_MINB
-#define STRATUM_TRACE_MINB 1
+// Resident threads per SM the register allocation must allow (640: 96
+// registers a thread, as the batched trace).
+#ifndef STRATUM_DROPIN_OCC
+#define STRATUM_DROPIN_OCC 640
 #endif
 
 namespace st {
 
-__global__ void __launch_bounds__(64, STRATUM_TRACE_MINB) tracePrimaryK(const float* __restrict__ W, const float* __restrict__ N,
-                                                   const uint32_t* __restrict__ O, const float* __restrict__ C,
-                                                   float* Hit, float* Surface, int width, int height, int rowStart,
-                                                   int rowCount) {
+constexpr int kDropInThreads = 64;
+
+__global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_OCC / kDropInThreads)
+    tracePrimaryK(const float* __restrict__ W, const float* __restrict__ N, const uint32_t* __restrict__ O,
+                  const float* __restrict__ C, float* Hit, float* Surface, int width, int height, int rowStart,
+                  int rowCount) {
   __shared__ Camera cam;
   __shared__ uint32_t org[4];
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+  if (threadIdx.x == 0) {
     cam = makeCamera(C);
     for (int i = 0; i < 4; i++) org[i] = O[i];
   }
   __syncthreads();
-  int x = int(blockIdx.x * blockDim.x + threadIdx.x), y = rowStart + int(blockIdx.y * blockDim.y + threadIdx.y);
-  if (x >= width || y >= height || y >= rowStart + rowCount) return;
-  f3 rd = primaryDir(cam, x, y, width, height);
-  TraceResult r = traceRay(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd, 1.08f / float(height));
+  const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
+  const int x = int(blockIdx.x) * 8 + (lane & 7);
+  const int y = rowStart + int(blockIdx.y) * 8 + warp * 4 + (lane >> 3);
+  const bool active = x < width && y < height && y < rowStart + rowCount;
+  const f3 rd = primaryDir(cam, active ? x : 0, active ? y : 0, width, height);
+#ifdef STRATUM_DROPIN_PER_LANE
+  if (!active) return;
+  const TraceResult r = traceRay(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
+                                 1.08f / float(height));
+#else
+  __shared__ WarpStage stage[kDropInThreads / 32];
+  const TraceResult r = traceWarp(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
+                                  1.08f / float(height), active, stage[warp], groupCache(nullptr));
+  if (!active) return;
+#endif
   storeTrace(Hit, Surface, size_t(y) * width + x, r);
 }
 
@@ -40,7 +64,7 @@ extern "C" int stratum_tracePrimary(const float* World, const float* Nodes, cons
   int rows = rowCount < height - rowStart ? rowCount : height - rowStart;
   if (rows <= 0) return STRATUM_OK;
   dim3 grid((width + 7) / 8, (rows + 7) / 8);
-  tracePrimaryK<<<grid, dim3(8, 8), 0, asStream(stream)>>>(World, Nodes, Origin, C, Hit, Surface, width, height,
-                                                         rowStart, rowCount);
+  tracePrimaryK<<<grid, kDropInThreads, 0, asStream(stream)>>>(World, Nodes, Origin, C, Hit, Surface, width, height,
+                                                             rowStart, rowCount);
   return launchStatus();
 }
