@@ -97,14 +97,24 @@ template <class R> R fbm2(R x, R y) {
 }
 template <class R> inline R freqWeight(R footprint, R freq) { return R(1) - smooth(R(0.35f), R(1.1f), footprint * freq); }
 
+// Sines and cosines of the camera and sun angles and of the resolve taps.
+// Mode 0 (default): the C library's float functions, as the reference's CPU
+// build calls them.  Mode 1: evaluated in double precision and rounded once to
+// float, as the CUDA path does; the C library's float functions are not always
+// correctly rounded (about 1.3 % of angles in [0, 2pi) differ by one ulp here),
+// so this mode gives the same ray basis as the device for every angle.
+int gAngleMode = 0;
+inline float angSin(float a) { return gAngleMode ? float(std::sin(double(a))) : std::sin(a); }
+inline float angCos(float a) { return gAngleMode ? float(std::cos(double(a))) : std::cos(a); }
+
 // camera basis and rays (common.cu:54-70)
 inline V3f camForward(const float* C) {
-  return mk(std::sin(C[3]) * std::cos(C[4]), std::sin(C[4]), std::cos(C[3]) * std::cos(C[4]));
+  return mk(angSin(C[3]) * angCos(C[4]), angSin(C[4]), angCos(C[3]) * angCos(C[4]));
 }
-inline V3f camRight(const float* C) { return mk(std::cos(C[3]), 0.0f, -std::sin(C[3])); }
+inline V3f camRight(const float* C) { return mk(angCos(C[3]), 0.0f, -angSin(C[3])); }
 inline V3f camPos(const float* C) { return mk(C[0], C[1], C[2]); }
 inline V3f sunDir(const float* C) {
-  return unit(mk(std::cos(C[7]) * std::cos(C[8]), std::sin(C[8]), std::sin(C[7]) * std::cos(C[8])));
+  return unit(mk(angCos(C[7]) * angCos(C[8]), angSin(C[8]), angSin(C[7]) * angCos(C[8])));
 }
 inline float halton(int value, int base) {
   float inv = 1.0f / float(base), place = inv, r = 0.0f;
@@ -1239,8 +1249,8 @@ void resolvePixel(const float* Lin, float* Hist, uint32_t* Px, const float* C, c
     float radius = clampv(float(height) / (std::fmax(Hit[b], 0.5f) * 1.08f) * 0.8f, 3.0f, 28.0f);
     for (int k = 0; k < 8; k++) {
       float a = float(k) * kPi * 0.25f + 0.2f;
-      int xx = int(clampv(float(x) + std::cos(a) * radius, 0.0f, float(width - 1)));
-      int yy = int(clampv(float(y) + std::sin(a) * radius, 0.0f, float(height - 1)));
+      int xx = int(clampv(float(x) + angCos(a) * radius, 0.0f, float(width - 1)));
+      int yy = int(clampv(float(y) + angSin(a) * radius, 0.0f, float(height - 1)));
       int j = (yy * width + xx) * 4;
       if (int(Hit[j + 1]) != -10000) {
         V3f other = ro + primaryDir(C, xx, yy, width, height) * Hit[j], delta = other - point;
@@ -1375,6 +1385,12 @@ using namespace orc;
 
 extern "C" {
 
+void orc_setAngleRounding(int mode) { gAngleMode = mode ? 1 : 0; }
+void orc_cameraBasis(const float* C, float* out6) {
+  V3f f = camForward(C), r = camRight(C);
+  out6[0] = f.x; out6[1] = f.y; out6[2] = f.z; out6[3] = r.x; out6[4] = r.y; out6[5] = r.z;
+}
+int orc_angleRounding(void) { return gAngleMode; }
 void orc_offset_tag(const uint32_t* origin, int dx, int dz, uint32_t* out) {
   Addr a = shiftAddr(origin, dx, dz);
   out[0] = a.xl; out[1] = a.xh; out[2] = a.zl; out[3] = a.zh;

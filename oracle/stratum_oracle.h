@@ -38,6 +38,13 @@ enum {
   ORC_COUNTERS = 32
 };
 
+/* Sines and cosines of camera, sun and resolve-tap angles: 0 (default) = the C
+ * library's float functions, as the reference's CPU build; 1 = double precision
+ * rounded once to float, as the CUDA path.  Process-wide. */
+void orc_setAngleRounding(int mode);
+int orc_angleRounding(void);
+/* The camera's forward and right vectors under the current angle mode. */
+void orc_cameraBasis(const float* C, float* out6);
 void orc_offset_tag(const uint32_t* origin, int dx, int dz, uint32_t* out4);
 uint32_t orc_tag_hash(const uint32_t* tag4, int seed);
 uint32_t orc_hashU(uint32_t x);

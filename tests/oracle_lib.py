@@ -153,6 +153,10 @@ class Oracle(_Lib):
         L.orc_featureNormal_f64.argtypes = [f32p, f64p, f64p]
         L.orc_queryLot_exhaustive.restype = ct.c_float
         L.orc_queryLot_exhaustive.argtypes = [f32p, f32p, f32p, ct.c_float, ct.c_float, ct.POINTER(ct.c_int), f32p]
+        L.orc_setAngleRounding.argtypes = [ct.c_int]
+        L.orc_setAngleRounding.restype = None
+        L.orc_angleRounding.restype = ct.c_int
+        L.orc_cameraBasis.argtypes = [f32p, f32p]
         L.orc_retestFeatures.argtypes = [f32p, u32p, f32p, i32p, ct.c_int, f32p, ct.c_int]
         L.orc_reintersectF64.argtypes = [f32p, u32p, f32p, f32p, f32p, ct.c_int, ct.c_int, f64p, f64p, i32p, ct.c_int]
 
@@ -193,6 +197,26 @@ class Oracle(_Lib):
         out = np.zeros(3, np.float64)
         self.lib.orc_featureNormal_f64(np.ascontiguousarray(f10, np.float32), np.ascontiguousarray(pt, np.float64), out)
         return out
+
+    def angle_rounding(self, mode=None):
+        """Get (and with `mode`, set) how camera/sun/tap angles are evaluated: 0 = the C library's
+        float sinf/cosf (the reference's CPU build), 1 = double rounded once (the CUDA path)."""
+        old = self.lib.orc_angleRounding()
+        if mode is not None:
+            self.lib.orc_setAngleRounding(int(mode))
+        return old
+
+    def camera_basis(self, C, mode):
+        """Forward and right vectors of camera state C with angle mode `mode` (bits)."""
+        prev = self.angle_rounding(mode)
+        out = np.zeros(6, np.float32)
+        self.lib.orc_cameraBasis(np.ascontiguousarray(C, np.float32), out)
+        self.angle_rounding(prev)
+        return out
+
+    def basis_matches_reference(self, C):
+        """True when the device's camera basis equals the reference CPU build's for C."""
+        return bool(np.array_equal(self.camera_basis(C, 0).view(np.uint32), self.camera_basis(C, 1).view(np.uint32)))
 
     def retest_features(self, world, origin, rays, ids, nthreads=0):
         """[t, n.xyz] of feature ids[i] = (slot, fid) on ray i, in its lot frame as the trace forms it."""
@@ -254,6 +278,21 @@ class RefLib(_Lib):
 
     def resolve_rows(self, linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads=0):
         self.lib.ref_resolveRows(linear, history, pixels, C, hit, surface, w, h, row0, rows, nthreads)
+
+
+class device_angles:
+    """Within this block the oracle evaluates camera, sun and resolve-tap angles
+    as the CUDA path does (double precision rounded once to float)."""
+
+    def __init__(self, orc):
+        self.orc = orc
+
+    def __enter__(self):
+        self.prev = self.orc.angle_rounding(1)
+        return self.orc
+
+    def __exit__(self, *a):
+        self.orc.angle_rounding(self.prev)
 
 
 def ref_available() -> bool:

@@ -190,11 +190,12 @@ def test_step_camera_inputs(cuda, oracle):
     """stepCamera under 400 steps of random input (kernels/world.cu:64-92): move,
     look, boost, slow, wheel, bookmarks 1-6, sun, view cycle, exposure, shadow
     toggle, tour and resize reset, with varying dt.  After every step the 64-bit
-    Origin equals the oracle's bit for bit and C agrees within 2e-6 relative
-    (the camera's sines and cosines: the device rounds a double-precision value
-    once, the reference's CPU build uses the C library's float functions, which
-    can differ by an ulp); most steps are bit-identical.  The device state is
-    reset to the oracle's after each step so the comparison is per step."""
+    Origin equals the oracle's bit for bit, and C equals it bit for bit when the
+    oracle evaluates the camera's sines and cosines as the device does (double
+    precision, rounded once); against the reference CPU build's C-library float
+    functions, which can be one ulp off, C agrees within 2e-6 relative and most
+    steps are bit-identical.  The device state is reset to the oracle's after
+    each step so the comparison is per step."""
     import ctypes as ct
     from stratum_hyperdetail_b200 import call, ptr
     rng = np.random.default_rng(7)
@@ -225,9 +226,14 @@ def test_step_camera_inputs(cuda, oracle):
         dt = float(rng.choice([0.0, 1.0 / 60.0, 1.0 / 30.0, 0.25]))
         g.I.copy_(torch.from_numpy(I))
         o.I[:] = I
+        dev_C, dev_O = o.C.copy(), o.Origin.copy()
         call("stratum_stepCamera", ptr(g.C), ptr(g.Origin), ptr(g.I), dt, w, h, s())
+        with ol.device_angles(oracle):
+            oracle.f("stepCamera")(dev_C, dev_O, o.I, ct.c_float(dt), w, h)
         oracle.f("stepCamera")(o.C, o.Origin, o.I, ct.c_float(dt), w, h)
         gc = g.C.cpu().numpy()
+        assert np.array_equal(gc.view(np.uint32), dev_C.view(np.uint32)), (step, np.flatnonzero(gc != dev_C))
+        assert np.array_equal(u32(g.Origin), dev_O), step
         assert np.array_equal(u32(g.Origin), o.Origin), step
         assert np.allclose(gc, o.C, rtol=2e-6, atol=1e-7), (step, np.flatnonzero(gc != o.C))
         exact += int(np.array_equal(gc.view(np.uint32), o.C.view(np.uint32)))
