@@ -11,9 +11,11 @@
 // otherwise least recently used sessions that are idle (nothing queued in a
 // launched batch) are evicted.  Eviction snapshots what the future needs (camera
 // state, table origin, accumulation buffer) to pinned host memory (pinned when
-// the session is opened, not while the scheduler holds its lock) and frees the
-// device memory to the server's own memory pool, which keeps it mapped for the
-// next admission; re-admission clears only what must start at zero (camera,
+// the session is opened, not while the scheduler holds its lock) and returns
+// the device block to the server's arena: device memory taken in 4 GiB chunks
+// (only while the budget allows) and divided among sessions by a host-side
+// first-fit allocator, so admitting and evicting never call the driver's
+// allocator on the request path; re-admission clears only what must start at zero (camera,
 // input, table, tags; History when there is no snapshot), restores the
 // snapshot and rebuilds the table and hierarchy from the seed, so the session
 // continues exactly as if it had never left (the world is a pure function of
@@ -43,6 +45,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -95,6 +98,7 @@ struct Session {
   Layout lay;
   char* base = nullptr;
   bool resident = false, inflight = false, started = false, restart = false;
+  bool admitQueued = false;  // admission work on the admission stream not yet waited for by a batch
   std::deque<Request*> queue;
   stratum_pose last{};
   double lastUse = 0.0;
@@ -134,6 +138,67 @@ struct Slot {
 
 bool samePose(const stratum_pose& a, const stratum_pose& b) { return std::memcmp(&a, &b, sizeof a) == 0; }
 
+// Session device memory: chunks of device memory taken with cudaMalloc while
+// the budget allows, each divided by first fit over a free list of (offset,
+// size) ranges that merges neighbours on release.  Blocks are multiples of
+// 2 MiB.  Only the scheduler thread (under the server lock) touches it.
+struct Arena {
+  struct Chunk {
+    char* base;
+    size_t size;
+    std::map<size_t, size_t> free;  // offset -> size, disjoint, not adjacent
+  };
+  static constexpr size_t kGrain = size_t(2) << 20;
+  static constexpr size_t kChunk = size_t(4) << 30;
+  std::vector<Chunk> chunks;
+  size_t reserved = 0;  // bytes held in chunks
+
+  static size_t round(size_t n) { return (n + kGrain - 1) / kGrain * kGrain; }
+  char* take(size_t need) {
+    for (Chunk& c : chunks)
+      for (auto it = c.free.begin(); it != c.free.end(); ++it)
+        if (it->second >= need) {
+          const size_t off = it->first, rest = it->second - need;
+          c.free.erase(it);
+          if (rest) c.free[off + need] = rest;
+          return c.base + off;
+        }
+    return nullptr;
+  }
+  // A new chunk of max(kChunk, need) bytes, within `limit` bytes in total.
+  int grow(size_t need, size_t limit) {
+    const size_t size = std::max(kChunk, need);
+    if (reserved + size > limit) return STRATUM_QUEUE_STALLED;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, size);
+    if (e != cudaSuccess) { cudaGetLastError(); return -int(e); }
+    Chunk c{static_cast<char*>(p), size, {}};
+    c.free[0] = size;
+    chunks.push_back(std::move(c));
+    reserved += size;
+    return STRATUM_OK;
+  }
+  void give(char* p, size_t size) {
+    for (Chunk& c : chunks) {
+      if (p < c.base || p >= c.base + c.size) continue;
+      size_t off = size_t(p - c.base);
+      auto next = c.free.lower_bound(off);
+      if (next != c.free.end() && off + size == next->first) { size += next->second; next = c.free.erase(next); }
+      if (next != c.free.begin()) {
+        auto prev = std::prev(next);
+        if (prev->first + prev->second == off) { prev->second += size; return; }
+      }
+      c.free[off] = size;
+      return;
+    }
+  }
+  void release() {
+    for (Chunk& c : chunks) cudaFree(c.base);
+    chunks.clear();
+    reserved = 0;
+  }
+};
+
 }  // namespace
 
 struct stratum_server {
@@ -148,7 +213,7 @@ struct stratum_server {
   std::atomic<bool> stop{false};
   cudaStream_t admitStream = nullptr;
   cudaEvent_t admitDone = nullptr;  // recorded after each admission's device work
-  cudaMemPool_t pool = nullptr;     // session memory; keeps freed blocks mapped up to the budget
+  Arena arena;                      // session device memory, at most `budget` bytes
   std::unordered_map<int, std::unique_ptr<Session>> sessions;
   int nextSession = 1;
   std::unordered_map<long long, std::unique_ptr<Request>> requests;
@@ -189,11 +254,12 @@ int evict(stratum_server* S, Session& s) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s.snap, s.at<float>(s.lay.History), P * 16, cudaMemcpyDeviceToHost, S->admitStream);
   if (e != cudaSuccess) return -int(e);
-  cudaFreeAsync(s.base, S->admitStream);
+  // the block is reused by admissions queued after these copies on the same stream
+  S->arena.give(s.base, Arena::round(s.lay.total));
   s.base = nullptr;
   s.resident = false;
   s.hasSnap = true;
-  S->residentBytes -= s.lay.total;
+  S->residentBytes -= Arena::round(s.lay.total);
   S->evictions++;
   return STRATUM_OK;
 }
@@ -202,26 +268,30 @@ bool contains(const std::vector<Session*>& v, const Session* s) { return std::fi
 
 // Make `s` resident.  STRATUM_QUEUE_STALLED: no room yet (retry later).
 int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
-  const size_t need = s.lay.total;
+  const size_t need = Arena::round(s.lay.total);
   if (need > S->budget) return STRATUM_BUDGET_EXCEEDED;
-  while (S->residentBytes + need > S->budget) {
-    Session* victim = nullptr;
-    for (auto& kv : S->sessions) {
-      Session* p = kv.second.get();
-      if (p->resident && !p->inflight && !contains(batch, p) && (!victim || p->lastUse < victim->lastUse)) victim = p;
-    }
-    if (!victim) return STRATUM_QUEUE_STALLED;
-    int st = evict(S, *victim);
-    if (st != STRATUM_OK) return st;
-  }
   if (S->injectAllocFail > 0) {
     S->injectAllocFail--;
     return -int(cudaErrorMemoryAllocation);
   }
-  void* p = nullptr;
-  cudaError_t e = cudaMallocFromPoolAsync(&p, need, S->pool, S->admitStream);
-  if (e != cudaSuccess) return -int(e);
-  s.base = static_cast<char*>(p);
+  // A free block that fits; else a new chunk while the budget allows; else
+  // evict idle sessions, least recently used first, until a block fits.
+  char* p = nullptr;
+  while (!(p = S->arena.take(need))) {
+    int st = S->arena.grow(need, S->budget);
+    if (st == STRATUM_OK) continue;
+    if (st != STRATUM_QUEUE_STALLED && S->arena.reserved == 0) return st;
+    Session* victim = nullptr;
+    for (auto& kv : S->sessions) {
+      Session* q = kv.second.get();
+      if (q->resident && !q->inflight && !contains(batch, q) && (!victim || q->lastUse < victim->lastUse)) victim = q;
+    }
+    if (!victim) return STRATUM_QUEUE_STALLED;
+    st = evict(S, *victim);
+    if (st != STRATUM_OK) return st;
+  }
+  cudaError_t e = cudaSuccess;
+  s.base = p;
   // Only what is read before it is written starts at zero: camera, origin and
   // input, the table and its tags (every lot is then described and its
   // hierarchy built), and History unless a snapshot restores it.  Nodes, the
@@ -250,12 +320,13 @@ int admit(stratum_server* S, Session& s, const std::vector<Session*>& batch) {
     if (e != cudaSuccess) st = -int(e);
   }
   if (st != STRATUM_OK) {
-    cudaFreeAsync(s.base, S->admitStream);
+    S->arena.give(s.base, need);
     s.base = nullptr;
     return st;
   }
   s.resident = true;
   s.hasSnap = false;
+  s.admitQueued = true;
   S->residentBytes += need;
   S->admissions++;
   return STRATUM_OK;
@@ -285,10 +356,14 @@ int launch(stratum_server* S, Slot& sl, const std::vector<Request*>& reqs) {
     if (r->tStart < 0) r->tStart = t;
   }
   cudaStream_t st = sl.stream;
-  // sessions admitted for this batch: their allocation, initialisation and
-  // restored snapshot are ordered on the admission stream
-  cudaError_t e = cudaStreamWaitEvent(st, S->admitDone, 0);
+  // sessions admitted for this batch: their initialisation and restored
+  // snapshot are ordered on the admission stream, which this batch then waits
+  // for; a batch of sessions that were resident already does not wait on it
+  bool admitted = false;
+  for (Request* r : reqs) admitted |= S->sessions[r->session]->admitQueued;
+  cudaError_t e = admitted ? cudaStreamWaitEvent(st, S->admitDone, 0) : cudaSuccess;
   if (e != cudaSuccess) return -int(e);  // nothing queued yet
+  for (Request* r : reqs) S->sessions[r->session]->admitQueued = false;
   int s = enqueue(S, sl, reqs, n);
   if (s != STRATUM_OK) {
     deferFailure(sl, reqs, s);
@@ -436,9 +511,9 @@ void schedule(stratum_server* S) {
 }
 
 void freeSession(stratum_server* S, Session& s) {
-  if (s.resident) {
-    cudaFreeAsync(s.base, S->admitStream);
-    S->residentBytes -= s.lay.total;
+  if (s.resident) {  // an idle session: nothing of it is queued on a batch stream
+    S->arena.give(s.base, Arena::round(s.lay.total));
+    S->residentBytes -= Arena::round(s.lay.total);
     s.resident = false;
   }
   if (s.pinnedOut) cudaFreeHost(s.pinnedOut);
@@ -461,20 +536,6 @@ stratum_server* stratum_server_create(unsigned long long budget_bytes, int max_v
   if (tune) S->tune = *tune;
   if (cudaStreamCreateWithFlags(&S->admitStream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&S->admitDone, cudaEventDisableTiming) != cudaSuccess) {
-    stratum_server_destroy(S.release());
-    return nullptr;
-  }
-  // Session memory comes from the server's own pool, which keeps up to the
-  // budget mapped after a free: an eviction followed by an admission reuses
-  // the pages instead of returning them to the driver and mapping them again.
-  cudaMemPoolProps props{};
-  props.allocType = cudaMemAllocationTypePinned;
-  props.handleTypes = cudaMemHandleTypeNone;
-  props.location.type = cudaMemLocationTypeDevice;
-  props.location.id = S->device;
-  unsigned long long keep = budget_bytes;  // the attribute is a 64-bit count of bytes
-  if (cudaMemPoolCreate(&S->pool, &props) != cudaSuccess ||
-      cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
     stratum_server_destroy(S.release());
     return nullptr;
   }
@@ -519,6 +580,7 @@ void stratum_server_destroy(stratum_server* S) {
   }
   for (auto& kv : S->sessions) freeSession(S, *kv.second);
   if (S->admitStream) cudaStreamSynchronize(S->admitStream);
+  S->arena.release();
   for (Slot& sl : S->slots) {
     cudaFree(sl.scratch); cudaFree(sl.dViews); cudaFree(sl.dPoses); cudaFree(sl.dFlags);
     cudaFreeHost(sl.hViews); cudaFreeHost(sl.hPoses); cudaFreeHost(sl.hFlags);
@@ -527,7 +589,6 @@ void stratum_server_destroy(stratum_server* S) {
   }
   if (S->admitDone) cudaEventDestroy(S->admitDone);
   if (S->admitStream) cudaStreamDestroy(S->admitStream);
-  if (S->pool) cudaMemPoolDestroy(S->pool);
   delete S;
 }
 

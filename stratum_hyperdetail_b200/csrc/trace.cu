@@ -10,6 +10,17 @@
 // leaves in the reference's order with the same running best, so Hit and
 // Surface equal the per-thread traversal (traverse.cuh) bit for bit; building
 // with STRATUM_DROPIN_PER_LANE selects that per-thread form instead.
+//
+// A 64-row strip of a 1600-wide frame is ~1.1 waves of warps, so each strip
+// ends in a tail with most SMs idle.  Strips are independent, so each launch is
+// a programmatic dependent of the kernel before it on the stream: its blocks
+// may start while that kernel's last blocks still run.  Every block first waits
+// (griddepcontrol.wait) until the preceding grid has completed or signalled,
+// before it reads or writes anything, and then signals its own dependents at
+// once; a trace strip signals before its pixels are written, which is safe
+// because the next trace strip touches other pixels, and any other kernel that
+// follows (shade, resolve, the caller's own) is launched without the attribute
+// and so starts only after every strip has completed.
 #include "common_api.cuh"
 #include "traverse_coop.cuh"
 
@@ -29,6 +40,8 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_OCC / kDropInTh
                   int rowCount) {
   __shared__ Camera cam;
   __shared__ uint32_t org[4];
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (threadIdx.x == 0) {
     cam = makeCamera(C);
     for (int i = 0; i < 4; i++) org[i] = O[i];
@@ -63,8 +76,18 @@ extern "C" int stratum_tracePrimary(const float* World, const float* Nodes, cons
   if (rowStart < 0 || rowCount < 0) return STRATUM_EINVAL;
   int rows = rowCount < height - rowStart ? rowCount : height - rowStart;
   if (rows <= 0) return STRATUM_OK;
-  dim3 grid((width + 7) / 8, (rows + 7) / 8);
-  tracePrimaryK<<<grid, kDropInThreads, 0, asStream(stream)>>>(World, Nodes, Origin, C, Hit, Surface, width, height,
-                                                             rowStart, rowCount);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((width + 7) / 8, (rows + 7) / 8);
+  cfg.blockDim = dim3(kDropInThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = asStream(stream);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, tracePrimaryK, World, Nodes, static_cast<const uint32_t*>(Origin), C, Hit,
+                                     Surface, width, height, rowStart, rowCount);
+  if (e != cudaSuccess) return -int(e);
   return launchStatus();
 }
