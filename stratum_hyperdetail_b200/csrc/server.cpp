@@ -165,10 +165,11 @@ struct Arena {
         }
     return nullptr;
   }
-  // A new chunk of max(kChunk, need) bytes, within `limit` bytes in total.
+  // A new chunk of kChunk bytes, or what is left of `limit` if that is less,
+  // but never less than `need`.
   int grow(size_t need, size_t limit) {
-    const size_t size = std::max(kChunk, need);
-    if (reserved + size > limit) return STRATUM_QUEUE_STALLED;
+    if (reserved + need > limit) return STRATUM_QUEUE_STALLED;
+    const size_t size = std::max(need, std::min(kChunk, (limit - reserved) / kGrain * kGrain));
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, size);
     if (e != cudaSuccess) { cudaGetLastError(); return -int(e); }
