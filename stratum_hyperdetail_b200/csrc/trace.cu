@@ -1,15 +1,19 @@
 // tracePrimary drop-in (kernels/trace.cu:29-61 of the reference): every pixel of
-// a strip of rows, in 8x8 pixel blocks as the reference launches it.
+// a strip of rows.
 //
-// A block is two warps, each tracing one 8x4 tile with the warp-cooperative
-// traversal of the batched renderer (traverse_coop.cuh): lanes walk their own
-// rays to the hierarchy leaves, and the warp evaluates one (lot, group) at a
-// time for every lane waiting on it, the group's records built once by the
-// random-access grammar and staged in shared memory.  The drop-in has only the
-// reference's buffers, so there is no group cache.  Each ray still visits its
-// leaves in the reference's order with the same running best, so Hit and
-// Surface equal the per-thread traversal (traverse.cuh) bit for bit; building
-// with STRATUM_DROPIN_PER_LANE selects that per-thread form instead.
+// A block covers 16x16 pixels with eight warps, each tracing one 8x4 tile with
+// the warp-cooperative traversal of the batched renderer (traverse_coop.cuh):
+// lanes walk their own rays to the hierarchy leaves, and the warp evaluates one
+// (lot, group) at a time for every lane waiting on it.  The drop-in has only
+// the reference's buffers, so there is no table-wide group cache; instead the
+// block keeps the groups its warps build (by the random-access grammar) in a
+// shared-memory table, and a warp that needs a group another warp of the block
+// has built reads it from there (neighbouring tiles reach the same groups: on
+// the bench poses a 16x16 block needs 6-9x fewer group builds than its warps
+// would alone).  Each ray still visits its leaves in the reference's order with
+// the same running best, so Hit and Surface equal the per-thread traversal
+// (traverse.cuh) bit for bit; building with STRATUM_DROPIN_PER_LANE selects that
+// per-thread form instead.
 //
 // A 64-row strip of a 1600-wide frame is ~1.1 waves of warps, so each strip
 // ends in a tail with most SMs idle.  Strips are independent, so each launch is
@@ -21,23 +25,32 @@
 // because the next trace strip touches other pixels, and any other kernel that
 // follows (shade, resolve, the caller's own) is launched without the attribute
 // and so starts only after every strip has completed.
+#include <mutex>
+
 #include "common_api.cuh"
 #include "traverse_coop.cuh"
 
-// Resident threads per SM the register allocation must allow (640: 96
-// registers a thread, as the batched trace).
-#ifndef STRATUM_DROPIN_OCC
-#define STRATUM_DROPIN_OCC 640
+// Resident blocks of 256 threads per SM the register allocation must allow
+// (2: up to 128 registers a thread).
+#ifndef STRATUM_DROPIN_BLOCKS
+#define STRATUM_DROPIN_BLOCKS 2
 #endif
 
 namespace st {
 
-constexpr int kDropInThreads = 64;
+constexpr int kDropInThreads = 256;  // eight warps: 2 x 4 tiles of 8x4 pixels
+constexpr int kDropInW = 16, kDropInH = 16;
+struct DropInShared {
+  WarpStage stage[kDropInThreads / 32];
+  BlockCache cache;
+};
 
-__global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_OCC / kDropInThreads)
+__global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_BLOCKS)
     tracePrimaryK(const float* __restrict__ W, const float* __restrict__ N, const uint32_t* __restrict__ O,
                   const float* __restrict__ C, float* Hit, float* Surface, int width, int height, int rowStart,
                   int rowCount) {
+  extern __shared__ __align__(16) unsigned char dropInBytes[];
+  DropInShared& sh = *reinterpret_cast<DropInShared*>(dropInBytes);
   __shared__ Camera cam;
   __shared__ uint32_t org[4];
   asm volatile("griddepcontrol.wait;" ::: "memory");
@@ -46,10 +59,11 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_OCC / kDropInTh
     cam = makeCamera(C);
     for (int i = 0; i < 4; i++) org[i] = O[i];
   }
+  blockCacheInit(sh.cache);
   __syncthreads();
   const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
-  const int x = int(blockIdx.x) * 8 + (lane & 7);
-  const int y = rowStart + int(blockIdx.y) * 8 + warp * 4 + (lane >> 3);
+  const int x = int(blockIdx.x) * kDropInW + (warp & 1) * 8 + (lane & 7);
+  const int y = rowStart + int(blockIdx.y) * kDropInH + (warp >> 1) * 4 + (lane >> 3);
   const bool active = x < width && y < height && y < rowStart + rowCount;
   const f3 rd = primaryDir(cam, active ? x : 0, active ? y : 0, width, height);
 #ifdef STRATUM_DROPIN_PER_LANE
@@ -57,9 +71,8 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_OCC / kDropInTh
   const TraceResult r = traceRay(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
                                  1.08f / float(height));
 #else
-  __shared__ WarpStage stage[kDropInThreads / 32];
   const TraceResult r = traceWarp(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
-                                  1.08f / float(height), active, stage[warp], groupCache(nullptr));
+                                  1.08f / float(height), active, sh.stage[warp], groupCache(nullptr), &sh.cache);
   if (!active) return;
 #endif
   storeTrace(Hit, Surface, size_t(y) * width + x, r);
@@ -69,6 +82,10 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_OCC / kDropInTh
 
 using namespace st;
 
+namespace {
+constexpr int kSmemDevices = 64;
+}
+
 extern "C" int stratum_tracePrimary(const float* World, const float* Nodes, const unsigned* Origin, const float* C,
                                     float* Hit, float* Surface, int width, int height, int rowStart, int rowCount,
                                     stratum_stream_t stream) {
@@ -76,10 +93,16 @@ extern "C" int stratum_tracePrimary(const float* World, const float* Nodes, cons
   if (rowStart < 0 || rowCount < 0) return STRATUM_EINVAL;
   int rows = rowCount < height - rowStart ? rowCount : height - rowStart;
   if (rows <= 0) return STRATUM_OK;
+  static std::once_flag once[kSmemDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kSmemDevices) return STRATUM_EINVAL;
+  std::call_once(once[dev], [] {
+    cudaFuncSetAttribute(tracePrimaryK, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(DropInShared)));
+  });
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((width + 7) / 8, (rows + 7) / 8);
+  cfg.gridDim = dim3((width + kDropInW - 1) / kDropInW, (rows + kDropInH - 1) / kDropInH);
   cfg.blockDim = dim3(kDropInThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = sizeof(DropInShared);
   cfg.stream = asStream(stream);
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;

@@ -224,6 +224,57 @@ struct WarpStage {
   ChunkBox boxes[kKeys][kRunsPerGroup];
 };
 
+// Group records shared by the warps of one block, for a trace with no
+// table-wide group cache (the drop-in entry point).  Write-once for the
+// block's life: a warp that builds a group copies it into the next free entry
+// and then marks it ready; entries are never replaced, so a warp that finds a
+// ready entry reads the records in place.  Two warps that miss the same group
+// at once may both insert it (harmless).  At most 32 entries: one lane checks
+// each entry per lookup.
+#ifndef STRATUM_BLOCK_CACHE_ENTRIES
+#define STRATUM_BLOCK_CACHE_ENTRIES 24
+#endif
+constexpr int kBlockEntries = STRATUM_BLOCK_CACHE_ENTRIES;
+static_assert(kBlockEntries >= 1 && kBlockEntries <= 32, "one lane per block-cache entry");
+struct BlockCache {
+  StagedFeat feats[kBlockEntries][kEntryRecords];
+  ChunkBox boxes[kBlockEntries][kRunsPerGroup];
+  int key[kBlockEntries];
+  int count[kBlockEntries];
+  volatile int ready[kBlockEntries];
+  unsigned next;
+};
+// Every thread of the block calls this before any lookup (followed by a
+// block-wide barrier).
+SD void blockCacheInit(BlockCache& bc) {
+  for (int i = int(threadIdx.x); i < kBlockEntries; i += int(blockDim.x)) bc.ready[i] = 0;
+  if (threadIdx.x == 0) bc.next = 0u;
+}
+// The ready entry holding `key`, or -1.  Warp-collective.
+SD int blockCacheFind(const BlockCache& bc, int key) {
+  const int lane = int(threadIdx.x & 31);
+  const int ready = lane < kBlockEntries ? bc.ready[lane] : 0;
+  // an entry's key and records were written before its ready flag: read them after it
+  __threadfence_block();
+  const bool hit = ready != 0 && reinterpret_cast<const volatile int*>(bc.key)[lane] == key;
+  const unsigned m = __ballot_sync(0xffffffffu, hit);
+  return m ? __ffs(m) - 1 : -1;
+}
+// Copy the group just staged in slot 0 of `ws` into a free entry, if any.  Warp-collective.
+SD void blockCachePut(BlockCache& bc, const WarpStage& ws, int key, int count) {
+  const int lane = int(threadIdx.x & 31);
+  unsigned e = 0u;
+  if (lane == 0) e = atomicAdd(&bc.next, 1u);
+  e = __shfl_sync(0xffffffffu, e, 0);
+  if (e >= unsigned(kBlockEntries)) return;
+  for (int k = lane; k < count; k += 32) bc.feats[e][k] = ws.feats[0][k];
+  if (lane < (count + kRun - 1) / kRun) bc.boxes[e][lane] = ws.boxes[0][lane];
+  if (lane == 0) { bc.key[e] = key; bc.count[e] = count; }
+  __syncwarp();
+  __threadfence_block();
+  if (lane == 0) bc.ready[e] = 1;
+}
+
 // Stage one group into slot q of the warp's stage: its records from the group
 // cache, or built by the grammar (and stored when the cache gives an entry),
 // and the chunk boxes.  Warp-collective; returns the group's record count.
@@ -282,7 +333,8 @@ SD int stageGroup(const float* __restrict__ W, const GroupCache& cache, int key,
 // (inactive lanes with active = false).  `ws` is this warp's shared-memory
 // staging area; `cache` is the table's group cache (null base: none).
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
-                         f3 rd, float cone, bool active, WarpStage& ws, const GroupCache& cache) {
+                         f3 rd, float cone, bool active, WarpStage& ws, const GroupCache& cache,
+                         BlockCache* bc = nullptr) {
   const int lane = int(threadIdx.x & 31);
   CoopRay r;
   coopBegin(r, ro, rd, cone, active);
@@ -298,6 +350,8 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
       // key first), staged one after another
       unsigned batch = 0u;
       int myq = -1, myCount = 0;
+      const StagedFeat* myFeats = nullptr;
+      const ChunkBox* myBoxes = nullptr;
 #pragma unroll
       for (int q = 0; q < kKeys; q++) {
         const unsigned rem = pending & ~batch;
@@ -305,8 +359,22 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
         const int key = __shfl_sync(0xffffffffu, myKey, __ffs(rem) - 1);
         const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && myKey == key);
         batch |= peers;
-        const int count = stageGroup(W, cache, key, ws, q);
-        if ((peers >> lane) & 1u) { myq = q; myCount = count; }
+        int count;
+        const StagedFeat* feats = ws.feats[q];
+        const ChunkBox* boxes = ws.boxes[q];
+        const int e = bc ? blockCacheFind(*bc, key) : -1;
+        if (e >= 0) {  // built earlier by a warp of this block
+          count = bc->count[e];
+          feats = bc->feats[e];
+          boxes = bc->boxes[e];
+        } else {
+          count = stageGroup(W, cache, key, ws, q);
+          if (bc && q == 0) {
+            __syncwarp();
+            blockCachePut(*bc, ws, key, count);
+          }
+        }
+        if ((peers >> lane) & 1u) { myq = q; myCount = count; myFeats = feats; myBoxes = boxes; }
       }
       __syncwarp();
       // every waiting lane tests its own group's records in index order
@@ -314,13 +382,13 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
         const int g = r.pend;
 #pragma unroll 1
         for (int c = 0; c * kRun < myCount; c++) {
-          const ChunkBox b = ws.boxes[myq][c];
+          const ChunkBox b = myBoxes[c];
           const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
           if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
           const int kEnd = min(myCount, (c + 1) * kRun);
 #pragma unroll 1
           for (int k = c * kRun; k < kEnd; k++) {
-            const Feat f = unstage(ws.feats[myq][k]);
+            const Feat f = unstage(myFeats[k]);
             const bool odd = f.turn % 2 == 1;
             const f3 inv = odd ? inv1Of(r) : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
             const Span rg = featureSlab(f, p, inv);
