@@ -30,16 +30,24 @@
 #include "common_api.cuh"
 #include "traverse_coop.cuh"
 
-// Resident blocks of 256 threads per SM the register allocation must allow
-// (2: up to 128 registers a thread).
+// Block shape in 8x4-pixel warp tiles, and resident blocks per SM the register
+// allocation must allow (2 blocks of 2 x 4 tiles: 512 threads, up to 128
+// registers a thread).
+#ifndef STRATUM_DROPIN_TILES_X
+#define STRATUM_DROPIN_TILES_X 2
+#endif
+#ifndef STRATUM_DROPIN_TILES_Y
+#define STRATUM_DROPIN_TILES_Y 4
+#endif
 #ifndef STRATUM_DROPIN_BLOCKS
 #define STRATUM_DROPIN_BLOCKS 2
 #endif
 
 namespace st {
 
-constexpr int kDropInThreads = 256;  // eight warps: 2 x 4 tiles of 8x4 pixels
-constexpr int kDropInW = 16, kDropInH = 16;
+constexpr int kDropInTilesX = STRATUM_DROPIN_TILES_X, kDropInTilesY = STRATUM_DROPIN_TILES_Y;
+constexpr int kDropInThreads = 32 * kDropInTilesX * kDropInTilesY;
+constexpr int kDropInW = 8 * kDropInTilesX, kDropInH = 4 * kDropInTilesY;
 struct DropInShared {
   WarpStage stage[kDropInThreads / 32];
   BlockCache cache;
@@ -62,8 +70,8 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_BLOCKS)
   blockCacheInit(sh.cache);
   __syncthreads();
   const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
-  const int x = int(blockIdx.x) * kDropInW + (warp & 1) * 8 + (lane & 7);
-  const int y = rowStart + int(blockIdx.y) * kDropInH + (warp >> 1) * 4 + (lane >> 3);
+  const int x = int(blockIdx.x) * kDropInW + (warp % kDropInTilesX) * 8 + (lane & 7);
+  const int y = rowStart + int(blockIdx.y) * kDropInH + (warp / kDropInTilesX) * 4 + (lane >> 3);
   const bool active = x < width && y < height && y < rowStart + rowCount;
   const f3 rd = primaryDir(cam, active ? x : 0, active ? y : 0, width, height);
 #ifdef STRATUM_DROPIN_PER_LANE

@@ -232,7 +232,7 @@ struct WarpStage {
 // at once may both insert it (harmless).  At most 32 entries: one lane checks
 // each entry per lookup.
 #ifndef STRATUM_BLOCK_CACHE_ENTRIES
-#define STRATUM_BLOCK_CACHE_ENTRIES 24
+#define STRATUM_BLOCK_CACHE_ENTRIES 32
 #endif
 constexpr int kBlockEntries = STRATUM_BLOCK_CACHE_ENTRIES;
 static_assert(kBlockEntries >= 1 && kBlockEntries <= 32, "one lane per block-cache entry");
