@@ -15,16 +15,13 @@
 // (traverse.cuh) bit for bit; building with STRATUM_DROPIN_PER_LANE selects that
 // per-thread form instead.
 //
-// A 64-row strip of a 1600-wide frame is ~1.1 waves of warps, so each strip
-// ends in a tail with most SMs idle.  Strips are independent, so each launch is
-// a programmatic dependent of the kernel before it on the stream: its blocks
-// may start while that kernel's last blocks still run.  Every block first waits
-// (griddepcontrol.wait) until the preceding grid has completed or signalled,
-// before it reads or writes anything, and then signals its own dependents at
-// once; a trace strip signals before its pixels are written, which is safe
-// because the next trace strip touches other pixels, and any other kernel that
-// follows (shade, resolve, the caller's own) is launched without the attribute
-// and so starts only after every strip has completed.
+// The reference's 64-row strips leave each launch a tail of partly idle SMs:
+// six 1600x900 views in 15 strips each trace in 24.4 ms, in one call per view
+// (rowCount = height, which the entry point accepts) in 14.3 ms.  A
+// programmatic dependent launch of each strip was tried and measured no
+// faster: a dependent grid may be scheduled early, but its griddepcontrol.wait
+// returns only once the preceding grid has completed, and skipping that wait is
+// safe only when the preceding kernel is known to be another strip.
 #include <mutex>
 
 #include "common_api.cuh"
@@ -61,8 +58,6 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_BLOCKS)
   DropInShared& sh = *reinterpret_cast<DropInShared*>(dropInBytes);
   __shared__ Camera cam;
   __shared__ uint32_t org[4];
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   if (threadIdx.x == 0) {
     cam = makeCamera(C);
     for (int i = 0; i < 4; i++) org[i] = O[i];
@@ -79,8 +74,9 @@ __global__ void __launch_bounds__(kDropInThreads, STRATUM_DROPIN_BLOCKS)
   const TraceResult r = traceRay(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
                                  1.08f / float(height));
 #else
-  const TraceResult r = traceWarp(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
-                                  1.08f / float(height), active, sh.stage[warp], groupCache(nullptr), &sh.cache);
+  const TraceResult r = traceWarp<true>(W, reinterpret_cast<const float4*>(N), org[0], org[2], cam.pos, rd,
+                                        1.08f / float(height), active, sh.stage[warp], groupCache(nullptr),
+                                        &sh.cache);
   if (!active) return;
 #endif
   storeTrace(Hit, Surface, size_t(y) * width + x, r);
@@ -107,18 +103,8 @@ extern "C" int stratum_tracePrimary(const float* World, const float* Nodes, cons
   std::call_once(once[dev], [] {
     cudaFuncSetAttribute(tracePrimaryK, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(DropInShared)));
   });
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((width + kDropInW - 1) / kDropInW, (rows + kDropInH - 1) / kDropInH);
-  cfg.blockDim = dim3(kDropInThreads);
-  cfg.dynamicSmemBytes = sizeof(DropInShared);
-  cfg.stream = asStream(stream);
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaError_t e = cudaLaunchKernelEx(&cfg, tracePrimaryK, World, Nodes, static_cast<const uint32_t*>(Origin), C, Hit,
-                                     Surface, width, height, rowStart, rowCount);
-  if (e != cudaSuccess) return -int(e);
+  dim3 grid((width + kDropInW - 1) / kDropInW, (rows + kDropInH - 1) / kDropInH);
+  tracePrimaryK<<<grid, kDropInThreads, sizeof(DropInShared), asStream(stream)>>>(
+      World, Nodes, static_cast<const uint32_t*>(Origin), C, Hit, Surface, width, height, rowStart, rowCount);
   return launchStatus();
 }

@@ -332,6 +332,9 @@ SD int stageGroup(const float* __restrict__ W, const GroupCache& cache, int key,
 // The whole warp traces its 32 rays.  Every lane of the warp must call this
 // (inactive lanes with active = false).  `ws` is this warp's shared-memory
 // staging area; `cache` is the table's group cache (null base: none).
+// kBlockCache: the block's warps share the groups they build through `bc`
+// (the drop-in trace); otherwise `bc` is unused.
+template <bool kBlockCache = false>
 SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__ N, uint32_t o0, uint32_t o2, f3 ro,
                          f3 rd, float cone, bool active, WarpStage& ws, const GroupCache& cache,
                          BlockCache* bc = nullptr) {
@@ -359,22 +362,27 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
         const int key = __shfl_sync(0xffffffffu, myKey, __ffs(rem) - 1);
         const unsigned peers = __ballot_sync(0xffffffffu, r.state == kLeafPending && myKey == key);
         batch |= peers;
-        int count;
-        const StagedFeat* feats = ws.feats[q];
-        const ChunkBox* boxes = ws.boxes[q];
-        const int e = bc ? blockCacheFind(*bc, key) : -1;
-        if (e >= 0) {  // built earlier by a warp of this block
-          count = bc->count[e];
-          feats = bc->feats[e];
-          boxes = bc->boxes[e];
-        } else {
-          count = stageGroup(W, cache, key, ws, q);
-          if (bc && q == 0) {
-            __syncwarp();
-            blockCachePut(*bc, ws, key, count);
+        if constexpr (kBlockCache) {
+          int count;
+          const StagedFeat* feats = ws.feats[q];
+          const ChunkBox* boxes = ws.boxes[q];
+          const int e = blockCacheFind(*bc, key);
+          if (e >= 0) {  // built earlier by a warp of this block
+            count = bc->count[e];
+            feats = bc->feats[e];
+            boxes = bc->boxes[e];
+          } else {
+            count = stageGroup(W, cache, key, ws, q);
+            if (q == 0) {
+              __syncwarp();
+              blockCachePut(*bc, ws, key, count);
+            }
           }
+          if ((peers >> lane) & 1u) { myq = q; myCount = count; myFeats = feats; myBoxes = boxes; }
+        } else {
+          const int count = stageGroup(W, cache, key, ws, q);
+          if ((peers >> lane) & 1u) { myq = q; myCount = count; }
         }
-        if ((peers >> lane) & 1u) { myq = q; myCount = count; myFeats = feats; myBoxes = boxes; }
       }
       __syncwarp();
       // every waiting lane tests its own group's records in index order
@@ -382,13 +390,13 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
         const int g = r.pend;
 #pragma unroll 1
         for (int c = 0; c * kRun < myCount; c++) {
-          const ChunkBox b = myBoxes[c];
+          const ChunkBox b = kBlockCache ? myBoxes[c] : ws.boxes[myq][c];
           const Span cr = slabInv(r.lr, r.inv0, mk(b.lo[0], b.lo[1], b.lo[2]), mk(b.hi[0], b.hi[1], b.hi[2]));
           if (cr.hi < fmaxf(0.001f, cr.lo) || cr.lo > r.best) continue;  // no feature of the run can win
           const int kEnd = min(myCount, (c + 1) * kRun);
 #pragma unroll 1
           for (int k = c * kRun; k < kEnd; k++) {
-            const Feat f = unstage(myFeats[k]);
+            const Feat f = unstage(kBlockCache ? myFeats[k] : ws.feats[myq][k]);
             const bool odd = f.turn % 2 == 1;
             const f3 inv = odd ? inv1Of(r) : r.inv0, p = intoFeature(r.lr - f.p, f.turn);
             const Span rg = featureSlab(f, p, inv);
