@@ -136,6 +136,32 @@ int stratum_traceRays(const float* World, const float* Nodes, const unsigned* Or
 int stratum_retestFeatures(const float* World, const unsigned* Origin, const float* Rays, const int* Ids, int n,
                            float* Out, stratum_stream_t stream);
 
+/* ---- optional material surrogate (kernels/learning.cu; the reference keeps it
+ * out of its build) --------------------------------------------------------
+ * An 8 -> 24 tanh -> 3 network (291 parameters W, Adam moments M and V) that
+ * learns the substrate colour of brick and stone from the frame's hit pixels;
+ * Brain[32] holds the step count, validation samples, errors, the gate
+ * Brain[4] and the last batch size.  Inputs come from the current buffers:
+ * Hit material and seed, Surface normal and slot, lot-frame masonry
+ * coordinates. */
+#define STRATUM_NN_PARAMS 291
+/* learning.cu:5-10: W, M, V (291 each) and Brain (32) from a seed. */
+int stratum_initNeural(float* W, float* M, float* V, float* Brain, int seed, stratum_stream_t stream);
+/* learning.cu:11-58 fused into one launch: on frames with C[6] % 4 == 0 and
+ * C[21] < 0.5, sample 64 brick/stone pixels, score the 8 held-out ones, update
+ * the gate and take one Adam step on the other 56.  Work (may be NULL) receives
+ * the 64 x 64 sample rows. */
+int stratum_materialStep(const float* World, const unsigned* Origin, const float* C, const float* Hit,
+                         const float* Surface, float* W, float* M, float* V, float* Brain, float* Work, int width,
+                         int height, stratum_stream_t stream);
+/* The surrogate's colour for n queries [u, v, seed, material] -> n x 3. */
+int stratum_predictSubstrate(const float* W, const float* Queries, int n, float* Out, stratum_stream_t stream);
+/* shadePixels with the surrogate for brick and stone when C[16] > 0.5 and
+ * Brain[4] > 0.5 (the reference's pre-refactor shade path), else identical. */
+int stratum_shadePixelsNeural(const float* World, const unsigned* Origin, const float* C, const float* Hit,
+                              const float* Surface, float* Linear, const float* W, const float* Brain, int width,
+                              int height, int rowStart, int rowCount, stratum_stream_t stream);
+
 /* ---- batched views (no reference counterpart: B200 multi-view form) ------- */
 /* One view of a batch: device pointers to that view's own buffers, in the
  * layouts above, plus its frame size and time step.  A batch is a DEVICE array

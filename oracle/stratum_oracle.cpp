@@ -106,6 +106,9 @@ template <class R> inline R freqWeight(R footprint, R freq) { return R(1) - smoo
 int gAngleMode = 0;
 inline float angSin(float a) { return gAngleMode ? float(std::sin(double(a))) : std::sin(a); }
 inline float angCos(float a) { return gAngleMode ? float(std::cos(double(a))) : std::cos(a); }
+// The material surrogate's exponentials and powers follow the same switch.
+inline float angExp(float x) { return gAngleMode ? float(std::exp(double(x))) : std::exp(x); }
+inline float angPow(float x, float y) { return gAngleMode ? float(std::pow(double(x), double(y))) : std::pow(x, y); }
 
 // camera basis and rays (common.cu:54-70)
 inline V3f camForward(const float* C) {
@@ -972,6 +975,44 @@ V3f substrate(float u, float v, float seed, int m) {
   float age = 0.61f + 0.52f * large, damp = smooth(0.49f, 0.76f, run) * 0.31f;
   return base * (age - damp) + mk(0.017f, 0.024f, 0.014f) * damp;
 }
+// ---- optional material surrogate (learning.cu; Stratum.cu:648-664) ---------
+// An 8 -> 24 tanh -> 3 network for the substrate colour of brick and stone.
+constexpr int kNnInputs = 8, kNnHidden = 24, kNnParams = 291, kNnBatch = 64, kNnWs = 64, kNnTrain = 56;
+constexpr int kNnB1 = 192, kNnW2 = 216, kNnB2 = 288;
+constexpr int kNnTarget = 8, kNnOut = 11, kNnHid = 14, kNnValid = 62, kNnMat = 63;
+inline bool materialTrainNow(const float* C) { return (int(C[6]) % 4) == 0 && C[21] < 0.5f; }  // learning.cu:4
+float nnFeature(int i, float u, float v, float seed, int mat) {  // Stratum.cu:648-657
+  if (i == 0) return angSin(u * 0.13f);
+  if (i == 1) return angCos(u * 0.13f);
+  if (i == 2) return angSin(v * 0.13f);
+  if (i == 3) return angCos(v * 0.13f);
+  if (i == 4) return noise2(u * 0.31f + seed * 0.013f, v * 0.31f) * 2.0f - 1.0f;
+  if (i == 5) return noise2(u * 0.42f + seed * 0.01f, v * 0.038f + 1.7f) * 2.0f - 1.0f;
+  if (i == 6) return float(mat) * 2.0f - 1.0f;
+  return angSin(seed * 0.03f);
+}
+inline float nnActivate(float x) {  // Stratum.cu:658
+  x = clampv(x, -8.0f, 8.0f);
+  return 2.0f / (1.0f + angExp(-2.0f * x)) - 1.0f;
+}
+V3f predictSubstrateNet(const float* W, float u, float v, float seed, int mat) {  // Stratum.cu:659-664
+  float hidden[kNnHidden];
+  for (int h = 0; h < kNnHidden; h++) {
+    float z = W[kNnB1 + h];
+    for (int j = 0; j < kNnInputs; j++) z += W[h * 8 + j] * nnFeature(j, u, v, seed, mat);
+    hidden[h] = nnActivate(z);
+  }
+  V3f out = mk(W[kNnB2], W[kNnB2 + 1], W[kNnB2 + 2]);
+  for (int h = 0; h < kNnHidden; h++) {
+    out.x += W[kNnW2 + h] * hidden[h];
+    out.y += W[kNnW2 + 24 + h] * hidden[h];
+    out.z += W[kNnW2 + 48 + h] * hidden[h];
+  }
+  return mk(sat(out.x), sat(out.y), sat(out.z));
+}
+// The surrogate's parameters while orc_shadePixelsNeural shades with it.
+const float* gNeuralW = nullptr;
+
 V3f skyColor(V3f rd, V3f sun) {
   float elev = sat(rd.y);
   V3f c = mix(mk(0.62f, 0.69f, 0.72f), mk(0.13f, 0.30f, 0.52f), std::pow(elev, 0.45f));
@@ -1172,7 +1213,7 @@ void shadePixel(const float* W, const uint32_t* O, const float* C, const float* 
     float u, v;
     masonryUV(q, qn, u, v);
     V3f base = substrateMean(mat);
-    if (mat == 0 || mat == 1) base = substrate(u, v, seed, mat);
+    if (mat == 0 || mat == 1) base = gNeuralW ? predictSubstrateNet(gNeuralW, u, v, seed, mat) : substrate(u, v, seed, mat);
     V3f albedo = surfaceColor(q, qn, mat, seed, sfp, base) * paletteTint(palette, mat);
     V3f originalN = n;
     if ((mat == 0 || mat == 1) && std::fabs(qn.y) < 0.5f) {
@@ -1584,6 +1625,146 @@ void orc_traceRays(const float* W, const float* N, const uint32_t* O, const floa
     const float* q = rays + size_t(i) * 7;
     traceRayOrc(W, N, O, mk(q[0], q[1], q[2]), mk(q[3], q[4], q[5]), q[6], exhaustive != 0, out + size_t(i) * 8);
   }
+}
+// learning.cu:5-10
+void orc_initNeural(float* W, float* M, float* V, float* Brain, int seed) {
+  for (int i = 0; i < kNnParams; i++) {
+    W[i] = (hash1(i + seed) - 0.5f) * 0.08f;
+    M[i] = 0.0f;
+    V[i] = 0.0f;
+    if (i >= kNnW2) W[i] = 0.0f;
+  }
+  for (int i = 0; i < 32; i++) Brain[i] = 0.0f;
+  W[kNnB2] = 0.36f; W[kNnB2 + 1] = 0.29f; W[kNnB2 + 2] = 0.20f;
+}
+// learning.cu:11-58, the five kernels in order; the sample's inputs come from
+// the current buffers (Hit material and seed, the lot-frame masonry
+// coordinates of shade.cu:54-65).
+void orc_materialStep(const float* Wd, const uint32_t* O, const float* C, const float* Hit, const float* Surf,
+                      float* W, float* M, float* V, float* Brain, float* WorkOut, int width, int height) {
+  if (!materialTrainNow(C)) return;
+  std::vector<float> work(kNnBatch * kNnWs, 0.0f);
+  const V3f ro = camPos(C);
+  for (int i = 0; i < kNnBatch; i++) {  // prepareMaterialBatch
+    float* w = work.data() + i * kNnWs;
+    int chosen = -1;
+    for (int trial = 0; trial < 6; trial++) {
+      const int px = int(hash1(i * 1877 + trial * 331 + int(C[6]) * 59) * float(width * height));
+      const int id = int(Hit[px * 4 + 1]);
+      if (id >= 0) {
+        const int mat = int(Hit[px * 4 + 2]);
+        if (mat == 0 || mat == 1) chosen = px;
+      }
+    }
+    if (chosen < 0) continue;
+    const int b = chosen * 4, x = chosen % width, y = chosen / width;
+    const V3f rd = primaryDir(C, x, y, width, height);
+    const V3f pt = ro + rd * Hit[b], n = mk(Surf[b], Surf[b + 1], Surf[b + 2]);
+    const int mat = int(Hit[b + 2]), slot = int(Surf[b + 3]);
+    const float seed = Hit[b + 3];
+    const LotDesc lot = loadLot(Wd, slot);
+    int cx, cz;
+    slotCell(O, slot, cx, cz);
+    const V3f cp = mk(float(cx) * kCell, 0.0f, float(cz) * kCell) + mk(lot.ox, 0.0f, lot.oz);
+    V3f q = toLot(pt - cp, lot.turn), qn = toLot(n, lot.turn);
+    float u, v;
+    masonryUV(q, qn, u, v);
+    for (int j = 0; j < kNnInputs; j++) w[j] = nnFeature(j, u, v, seed, mat);
+    const V3f target = substrate(u, v, seed, mat);
+    w[kNnTarget] = target.x; w[kNnTarget + 1] = target.y; w[kNnTarget + 2] = target.z;
+    w[kNnValid] = 1.0f;
+    w[kNnMat] = float(mat);
+  }
+  for (int i = 0; i < kNnBatch; i++) {  // materialForward
+    float* w = work.data() + i * kNnWs;
+    for (int h = 0; h < kNnHidden; h++) {
+      float z = W[kNnB1 + h];
+      for (int j = 0; j < kNnInputs; j++) z += W[h * 8 + j] * w[j];
+      w[kNnHid + h] = nnActivate(z);
+    }
+    for (int o = 0; o < 3; o++) {
+      float z = W[kNnB2 + o];
+      for (int h = 0; h < kNnHidden; h++) z += W[kNnW2 + o * 24 + h] * w[kNnHid + h];
+      w[kNnOut + o] = z;
+    }
+  }
+  {  // scoreMaterial
+    float err = 0.0f, baseline = 0.0f, n = 0.0f;
+    for (int k = kNnTrain; k < kNnBatch; k++) {
+      const float* w = work.data() + k * kNnWs;
+      if (w[kNnValid] > 0.5f) {
+        n += 1.0f;
+        const V3f mean = substrateMean(int(w[kNnMat]));
+        for (int o = 0; o < 3; o++) {
+          const float d = w[kNnOut + o] - w[kNnTarget + o];
+          err += d * d;
+          const float m = o == 0 ? mean.x : (o == 1 ? mean.y : mean.z);
+          const float e = m - w[kNnTarget + o];
+          baseline += e * e;
+        }
+      }
+    }
+    if (n > 0.0f) {
+      const float a = Brain[1] < 1.0f ? 1.0f : 0.065f;
+      Brain[2] = lerp(Brain[2], err / (n * 3.0f), a);
+      Brain[3] = lerp(Brain[3], baseline / (n * 3.0f), a);
+      Brain[1] += n;
+    }
+    Brain[4] = Brain[1] >= 256.0f && Brain[2] < Brain[3] * 0.90f && Brain[2] < 0.0012f ? 1.0f : 0.0f;
+  }
+  float grad[kNnParams];
+  float count = 0.0f;
+  for (int i = 0; i < kNnParams; i++) {  // materialGradient
+    float g = 0.0f;
+    count = 0.0f;
+    for (int k = 0; k < kNnTrain; k++) {
+      const float* w = work.data() + k * kNnWs;
+      if (w[kNnValid] > 0.5f) {
+        count += 1.0f;
+        if (i < kNnW2) {
+          const int h = i < kNnB1 ? i / 8 : i - kNnB1;
+          float d = 0.0f;
+          for (int o = 0; o < 3; o++) d += (w[kNnOut + o] - w[kNnTarget + o]) * W[kNnW2 + o * 24 + h];
+          const float a = w[kNnHid + h];
+          d *= 1.0f - a * a;
+          g += i < kNnB1 ? d * w[i % 8] : d;
+        } else if (i < kNnB2) {
+          const int o = (i - kNnW2) / 24, h = (i - kNnW2) % 24;
+          g += (w[kNnOut + o] - w[kNnTarget + o]) * w[kNnHid + h];
+        } else {
+          const int o = i - kNnB2;
+          g += w[kNnOut + o] - w[kNnTarget + o];
+        }
+      }
+    }
+    grad[i] = clampv(g / std::fmax(1.0f, count), -0.8f, 0.8f);
+  }
+  if (count > 0.0f) Brain[0] += 1.0f;
+  Brain[5] = count;
+  if (Brain[5] >= 1.0f)  // materialAdam
+    for (int i = 0; i < kNnParams; i++) {
+      const float g = grad[i];
+      const float m = 0.9f * M[i] + 0.1f * g, v = 0.999f * V[i] + 0.001f * g * g;
+      M[i] = m;
+      V[i] = v;
+      const float mh = m / (1.0f - angPow(0.9f, Brain[0])), vh = v / (1.0f - angPow(0.999f, Brain[0]));
+      W[i] -= 0.002f * (mh / (std::sqrt(vh) + 0.00001f) + 0.0001f * W[i]);
+    }
+  if (WorkOut) std::memcpy(WorkOut, work.data(), sizeof(float) * work.size());
+}
+void orc_predictSubstrate(const float* W, const float* Q, int n, float* out) {
+  for (int i = 0; i < n; i++) {
+    const V3f c = predictSubstrateNet(W, Q[i * 4], Q[i * 4 + 1], Q[i * 4 + 2], int(Q[i * 4 + 3]));
+    out[i * 3] = c.x; out[i * 3 + 1] = c.y; out[i * 3 + 2] = c.z;
+  }
+}
+// shadePixels with the surrogate when C[16] > 0.5 and Brain[4] > 0.5 (Stratum.cu:854).
+void orc_shadePixelsNeural(const float* Wd, const uint32_t* O, const float* C, const float* Hit, const float* Surf,
+                           float* Lin, const float* W, const float* Brain, int width, int height, int rowStart,
+                           int rowCount, int nthreads) {
+  gNeuralW = C[16] > 0.5f && Brain[4] > 0.5f ? W : nullptr;
+  orc_shadePixels(Wd, O, C, Hit, Surf, Lin, width, height, rowStart, rowCount, nthreads, nullptr);
+  gNeuralW = nullptr;
 }
 // trace, shade and resolve of the listed rows only, in parallel over pixels.
 void orc_renderRows(const float* W, const float* N, const uint32_t* O, const float* C, float* Hit, float* Surf,

@@ -84,6 +84,17 @@ void orc_traceRays(const float* World, const float* Nodes, const uint32_t* Origi
 void orc_resolveRows(const float* Linear, float* History, uint32_t* Pixels, const float* C, const float* Hit,
                      const float* Surface, int width, int height, int rowStart, int rowCount, int nthreads);
 void orc_probeGrammar(const float* Inputs, float* Output);
+/* The optional material surrogate (learning.cu): init, one training step
+ * (Work: 64 x 64 sample rows, may be NULL), the surrogate colour of n queries
+ * [u, v, seed, material] -> n x 3, and shadePixels with the surrogate. */
+void orc_initNeural(float* W, float* M, float* V, float* Brain, int seed);
+void orc_materialStep(const float* World, const uint32_t* Origin, const float* C, const float* Hit,
+                      const float* Surface, float* W, float* M, float* V, float* Brain, float* Work, int width,
+                      int height);
+void orc_predictSubstrate(const float* W, const float* Queries, int n, float* out);
+void orc_shadePixelsNeural(const float* World, const uint32_t* Origin, const float* C, const float* Hit,
+                           const float* Surface, float* Linear, const float* W, const float* Brain, int width,
+                           int height, int rowStart, int rowCount, int nthreads);
 /* trace + shade + resolve of the listed rows (rows[nrows]) only. */
 void orc_renderRows(const float* World, const float* Nodes, const uint32_t* Origin, const float* C, float* Hit,
                     float* Surface, float* Linear, float* History, uint32_t* Pixels, int width, int height,

@@ -25,6 +25,7 @@ BUILD_CHUNK = 2048
 BUILD_CHUNKS = 8
 RAY_DISTANCE = 2000.0
 SKY_ID = -10000
+NN_PARAMS = 291
 GROUND_ID = -1
 
 OK = 0
@@ -70,6 +71,10 @@ SIGNATURES: dict[str, list] = {
     "stratum_featureQuery": [_P, _I, _P, _S],
     "stratum_traceRays": [_P, _P, _P, _P, _I, _I, _P, _S],
     "stratum_retestFeatures": [_P, _P, _P, _P, _I, _P, _S],
+    "stratum_initNeural": [_P, _P, _P, _P, _I, _S],
+    "stratum_materialStep": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _S],
+    "stratum_predictSubstrate": [_P, _P, _I, _P, _S],
+    "stratum_shadePixelsNeural": [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _S],
     "stratum_applyPoses": [_P, _P, _P, _I, _S],
     "stratum_stepViews": [_P, _I, _S],
     "stratum_refreshViews": [_P, _I, _S],

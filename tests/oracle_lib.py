@@ -153,6 +153,11 @@ class Oracle(_Lib):
         L.orc_featureNormal_f64.argtypes = [f32p, f64p, f64p]
         L.orc_queryLot_exhaustive.restype = ct.c_float
         L.orc_queryLot_exhaustive.argtypes = [f32p, f32p, f32p, ct.c_float, ct.c_float, ct.POINTER(ct.c_int), f32p]
+        L.orc_initNeural.argtypes = [f32p, f32p, f32p, f32p, ct.c_int]
+        L.orc_materialStep.argtypes = [f32p, u32p, f32p, f32p, f32p, f32p, f32p, f32p, f32p, ct.c_void_p, ct.c_int,
+                                       ct.c_int]
+        L.orc_predictSubstrate.argtypes = [f32p, f32p, ct.c_int, f32p]
+        L.orc_shadePixelsNeural.argtypes = [f32p, u32p, f32p, f32p, f32p, f32p, f32p, f32p] + [ct.c_int] * 5
         L.orc_setAngleRounding.argtypes = [ct.c_int]
         L.orc_setAngleRounding.restype = None
         L.orc_angleRounding.restype = ct.c_int
@@ -205,6 +210,30 @@ class Oracle(_Lib):
         if mode is not None:
             self.lib.orc_setAngleRounding(int(mode))
         return old
+
+    # -- the optional material surrogate (learning.cu) ----------------------
+    def init_neural(self, seed):
+        """(W, M, V, Brain) of a fresh surrogate."""
+        W, M, V, B = np.zeros(291, np.float32), np.zeros(291, np.float32), np.zeros(291, np.float32), np.zeros(32, np.float32)
+        self.lib.orc_initNeural(W, M, V, B, int(seed))
+        return W, M, V, B
+
+    def material_step(self, s, hit, surface, net, width, height, work=None):
+        """One training step on a frame (s: World/Origin/C), updating net = (W, M, V, Brain) in place."""
+        W, M, V, B = net
+        self.lib.orc_materialStep(s.World, s.Origin, s.C, np.ascontiguousarray(hit, np.float32),
+                                  np.ascontiguousarray(surface, np.float32), W, M, V, B,
+                                  None if work is None else work.ctypes.data, int(width), int(height))
+
+    def predict_substrate(self, W, queries):
+        q = np.ascontiguousarray(queries, np.float32)
+        out = np.zeros((len(q), 3), np.float32)
+        self.lib.orc_predictSubstrate(W, q, len(q), out)
+        return out
+
+    def shade_neural(self, s, hit, surface, linear, W, brain, width, height, nthreads=0):
+        self.lib.orc_shadePixelsNeural(s.World, s.Origin, s.C, hit, surface, linear, W, brain, int(width), int(height),
+                                       0, int(height), nthreads)
 
     def camera_basis(self, C, mode):
         """Forward and right vectors of camera state C with angle mode `mode` (bits)."""
