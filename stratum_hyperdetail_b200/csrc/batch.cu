@@ -145,14 +145,14 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
   }
 }
 
-// STRATUM_TRACE_OCC / THREADS resident blocks (rounded down).  640 threads per
-// SM (96 registers per thread for 64- and 128-thread blocks, 128 for 256) and
-// 576 or 704 measured alike, 6-8 % faster than 768 (80 registers, heavy
-// spills) with the group cache in place.
+// STRATUM_TRACE_OCC / THREADS resident blocks (rounded down).  512 threads per
+// SM (128 registers, no spills): the six-view 1600x900 trace in 7.9 ms against
+// 8.3 ms at 640 (96 registers, 88/136 bytes of spills), every pose faster;
+// 768 (80 registers, heavy spills) is slower still.
 // The warp-cooperative traversal (traverse_coop.cuh) unless built with
 // STRATUM_BATCH_PER_LANE (each lane walks its own ray, as the drop-in kernel).
 #ifndef STRATUM_TRACE_OCC
-#define STRATUM_TRACE_OCC 640
+#define STRATUM_TRACE_OCC 512
 #endif
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
