@@ -11,6 +11,8 @@ drop-in path), through the C ABI.
   the same camera state over a table built from scratch for the same origin
   (the running History is handed to the oracle so the accumulation step is
   compared exactly).
+* Frames of 1x1, 7x3, 9x5, 33x17, 16,384 x 4 (the maximum width) and 3 x 2,000,
+  batched and through the drop-in strips, against the oracle.
 
 The oracle evaluates camera angles as the device does (double precision
 rounded once), so Hit and Surface must be bit-identical; colour within 1/1024.
@@ -104,3 +106,44 @@ def test_streaming_flight_frames_against_oracle(cuda, oracle):
         compared.append((frame, int(org[0]), int(org[1])))
     assert compared[0][1:] == (0, 1), compared  # the carry frame: xl wrapped to 0, xh incremented
     assert compared[-1][2] == 1, compared
+
+
+def test_tiny_ragged_and_extreme_frames_against_oracle(cuda, oracle):
+    """Frames smaller than one 8x4 tile, with ragged edges, and at the maximum
+    width (16,384 x 4) and a 3 x 2,000 column, rendered by the batched launch
+    and by the drop-in strips (64 rows, the last one asking for more rows than
+    remain), each against the oracle."""
+    import stratum_hyperdetail_b200 as sb
+    from stratum_hyperdetail_b200.batch import Batch
+    from stratum_hyperdetail_b200.views import View
+    sizes = [(1, 1), (7, 3), (9, 5), (33, 17), (16384, 4), (3, 2000)]
+    poses = [((3.0 * i, 1.7 + 9.0 * i, -2.0), 0.4 * i + 0.1, -0.05 * i) for i in range(len(sizes))]
+    views = []
+    for i, ((w, h), (pos, yaw, pitch)) in enumerate(zip(sizes, poses)):
+        v = View(w, h)
+        v.set_pose(100 + i, (i, 0, 2 * i, 0), pos, yaw, pitch)
+        v.C[19] = 1.0
+        views.append(v)
+    b = Batch(views, (64, 2, 1))
+    b.render()
+    torch.cuda.synchronize()
+    batched = [host_frame(v) for v in views]
+    s = torch.cuda.current_stream().cuda_stream
+    for v in views:
+        v.History.zero_()
+        w, h = v.width, v.height
+        for y in range(0, h, 64):
+            sb.call("stratum_tracePrimary", sb.ptr(v.World), sb.ptr(v.Nodes), sb.ptr(v.Origin), sb.ptr(v.C),
+                    sb.ptr(v.Hit), sb.ptr(v.Surface), w, h, y, 64, s)
+            sb.call("stratum_shadePixels", sb.ptr(v.World), sb.ptr(v.Origin), sb.ptr(v.C), sb.ptr(v.Hit),
+                    sb.ptr(v.Surface), sb.ptr(v.Linear), w, h, y, 64, s)
+        sb.call("stratum_resolveFrame", sb.ptr(v.Linear), sb.ptr(v.History), sb.ptr(v.Pixels), sb.ptr(v.C),
+                sb.ptr(v.Hit), sb.ptr(v.Surface), w, h, s)
+    torch.cuda.synchronize()
+    with ol.device_angles(oracle):
+        for i, ((w, h), (pos, yaw, pitch), v) in enumerate(zip(sizes, poses, views)):
+            o = ol.setup_pose(oracle, 100 + i, pos, yaw, pitch, w, h, origin=(i, 0, 2 * i, 0))
+            second = np.zeros(w * h, np.float32)
+            want = ol.render(oracle, o, w, h, second=second)
+            check(f"{w}x{h} batched", batched[i], want, second)
+            check(f"{w}x{h} drop-in", host_frame(v), want, second)
