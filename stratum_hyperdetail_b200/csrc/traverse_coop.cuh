@@ -79,6 +79,18 @@ SD void hitBox(const Feat& f, f3& lo, f3& hi) {
 
 enum LaneState : int { kEnterLot = 0, kInLot = 1, kLeafPending = 2, kDone = 3 };
 
+// Leaves a lane may find ahead in its lot before the warp evaluates them.  With
+// more than one, a lane that reaches a leaf keeps walking the lot's hierarchy
+// (near-first, against the best it has) and queues up to this many leaves; each
+// queued leaf is tested again against the lane's best when it comes up, so the
+// lane evaluates exactly the reference's leaves in the reference's order (a
+// leaf that passes has ancestors that pass: parents bound their children).
+#ifndef STRATUM_SPEC_LEAVES
+#define STRATUM_SPEC_LEAVES 4
+#endif
+constexpr int kSpec = STRATUM_SPEC_LEAVES;
+static_assert(kSpec >= 1 && kSpec <= 4, "up to four queued leaves (8 bits each in one word)");
+
 struct CoopRay {
   // ray and result
   f3 ro, rd;
@@ -94,6 +106,10 @@ struct CoopRay {
   unsigned long long stack;
   int node, qsteps, pend, state;
   int fresh;  // node's entry was just found nearer than best (by its parent's test)
+#if STRATUM_SPEC_LEAVES > 1
+  unsigned queue;  // queued leaves of the current lot: group indices, 8 bits each, the head lowest
+  int qn;
+#endif
 };
 
 SD int popNode(unsigned long long& stack) {
@@ -109,6 +125,9 @@ SD void coopBegin(CoopRay& r, f3 ro, f3 rd, float cone, bool active) {
   r.state = active ? kEnterLot : kDone;
   r.stack = 0ull; r.node = 0; r.qsteps = 0; r.pend = 0; r.slot = 0; r.lcx = r.lcz = 0; r.fresh = 0;
   r.ddaSteps = 0;
+#if STRATUM_SPEC_LEAVES > 1
+  r.queue = 0u; r.qn = 0;
+#endif
   if (!active) return;
   if (rd.y < -0.000001f) {
     float ground = -ro.y / rd.y;
@@ -158,7 +177,13 @@ SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __res
       }
       continue;
     }
-    if (r.node <= 0 || r.qsteps >= kNodes) { r.state = kEnterLot; continue; }
+    if (r.node <= 0 || r.qsteps >= kNodes) {
+#if STRATUM_SPEC_LEAVES > 1
+      if (r.qn > 0) { r.state = kLeafPending; r.pend = int(r.queue & 255u); break; }  // this lot's leaves first
+#endif
+      r.state = kEnterLot;
+      continue;
+    }
     r.qsteps++;
     const int base = r.slot * kNodes;
     // A node reached from its parent was tested against the same best a
@@ -179,7 +204,17 @@ SD void coopAdvance(CoopRay& r, const float* __restrict__ W, const float4* __res
       else if (rh) r.node = right;
       else r.node = popNode(r.stack);
     } else {
+#if STRATUM_SPEC_LEAVES > 1
+      if (near && r.node >= kGroups) {
+        r.queue |= unsigned(r.node - kGroups) << (8 * r.qn);
+        r.qn++;
+        r.node = popNode(r.stack);
+        if (r.qn == kSpec) { r.state = kLeafPending; r.pend = int(r.queue & 255u); break; }
+        continue;
+      }
+#else
       if (near && r.node >= kGroups) { r.state = kLeafPending; r.pend = r.node - kGroups; break; }
+#endif
       r.node = popNode(r.stack);
     }
   }
@@ -346,9 +381,16 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
     coopAdvance(r, W, N, o0, o2);
     unsigned pending = __ballot_sync(0xffffffffu, r.state == kLeafPending);
     if (!pending) break;  // every lane is done (lanes only stop advancing at a leaf or when done)
+#if STRATUM_SPEC_LEAVES > 1
+    static_assert(kKeys == 1, "queued leaves are served one group at a time");
+#pragma unroll 1
+    while (pending) {
+      const int myKey = (r.slot << 6) | r.pend;
+#else
     const int myKey = (r.slot << 6) | r.pend;
 #pragma unroll 1
     while (pending) {
+#endif
       // up to kKeys distinct keys of the pending lanes (first pending lane's
       // key first), staged one after another
       unsigned batch = 0u;
@@ -408,12 +450,30 @@ SD TraceResult traceWarp(const float* __restrict__ W, const float4* __restrict__
             }
           }
         }
+#if STRATUM_SPEC_LEAVES > 1
+        // the next queued leaf that can still win (its node tested against
+        // the best just found, as the reference tests it when it gets there)
+        r.queue >>= 8;
+        r.qn--;
+#pragma unroll 1
+        while (r.qn > 0 && !(nodeEntry(N, r.slot * kNodes + kGroups + int(r.queue & 255u), r.lr, r.inv0, r.best) < r.best)) {
+          r.queue >>= 8;
+          r.qn--;
+        }
+        if (r.qn > 0) r.pend = int(r.queue & 255u);
+        else r.state = kInLot;  // the walk goes on from where it stopped
+      }
+      __syncwarp();
+      pending = __ballot_sync(0xffffffffu, r.state == kLeafPending);
+    }
+#else
         r.state = kInLot;
         r.node = popNode(r.stack);
       }
       __syncwarp();
       pending &= ~batch;
     }
+#endif
   }
   TraceResult out;
   out.t = r.best; out.fid = r.fid; out.material = 10; out.seed = 0.0f; out.slot = -1;
