@@ -106,24 +106,9 @@ SD uint32_t tagWord(const float* row, int group, int count, int k) {
   return 0u;
 }
 
-// Warp-collective: the entry holding (slot, group) with this descriptor, or -1.
-// Every lane of the warp calls it with the same arguments.
-SD int cacheFind(const GroupCache& c, const float* W, int slot, int group, int count, uint32_t& word) {
-  word = 0u;
-  if (!c.base) return -1;
-  const int lane = int(threadIdx.x & 31);
-  word = __ldcg(c.dir(slot, group));
-  const int e = usableEntry(c, word);
-  if (e < 0) return -1;
-  bool same = true;
-  if (lane < kEntryTagWords)
-    same = __ldg(entryTag(c, uint32_t(e)) + lane) == tagWord(W + size_t(slot) * kLotFloats, group, count, lane);
-  return __all_sync(0xffffffffu, same) ? e : -1;
-}
-
 // Warp-collective: claim a fresh entry for (slot, group), or -1 when another
 // warp is filling it, filled it in this launch, or the store is full.  `old`
-// is the directory word cacheFind saw.  A claimed entry must be published.
+// is the directory word the caller read.  A claimed entry must be published.
 SD int cacheClaim(const GroupCache& c, int slot, int group, uint32_t old) {
   if (c.capacity() == 0u || old == kCacheBusy || (old != 0u && (old >> 24) == c.epoch())) return -1;
   int e = -1;

@@ -316,22 +316,37 @@ SD void blockCachePut(BlockCache& bc, const WarpStage& ws, int key, int count) {
 SD int stageGroup(const float* __restrict__ W, const GroupCache& cache, int key, WarpStage& ws, int q) {
   const int lane = int(threadIdx.x & 31);
   const int slot = key >> 6, g = key & 63;
+  // the directory word, the lot row, the entry's tag and its records in as few
+  // dependent round trips as possible: the records are loaded with the tag and
+  // kept only if every tag word matches the slot's current descriptor (else a miss)
+  uint32_t word = cache.base ? __ldcg(cache.dir(slot, g)) : 0u;
   const LotDesc L = loadLot(W, slot);
   const int count = groupCount(L, g);
-  uint32_t word;
-  int e = cacheFind(cache, W, slot, g, count, word);
-  const bool cached = e >= 0;
-  if (!cached) e = cacheClaim(cache, slot, g, word);  // -1: build without storing
-  if (cached) {  // records and chunk boxes as stored
-    if (lane < count) ws.feats[q][lane] = cacheRecord(cache, e, lane);
-    if (lane + 32 < count) ws.feats[q][lane + 32] = cacheRecord(cache, e, lane + 32);
+  int e = cache.base ? usableEntry(cache, word) : -1;
+  if (e >= 0) {
+    bool same = true;
+    if (lane < kEntryTagWords)
+      same = __ldg(entryTag(cache, uint32_t(e)) + lane) == tagWord(W + size_t(slot) * kLotFloats, g, count, lane);
+    StagedFeat r0{}, r1{};
+    if (lane < count) r0 = cacheRecord(cache, e, lane);
+    if (lane + 32 < count) r1 = cacheRecord(cache, e, lane + 32);
     const int runs = (count + kRun - 1) / kRun;
+    float2 ba{}, bb{}, bc{};
     if (lane < runs) {
       const float2* bp = reinterpret_cast<const float2*>(entryBoxes(cache, uint32_t(e)) + lane * 6);
-      const float2 a = __ldg(bp), b = __ldg(bp + 1), c = __ldg(bp + 2);
-      ws.boxes[q][lane] = ChunkBox{{a.x, a.y, b.x}, {b.y, c.x, c.y}};
+      ba = __ldg(bp); bb = __ldg(bp + 1); bc = __ldg(bp + 2);
     }
-  } else {
+    if (__all_sync(0xffffffffu, same)) {  // records and chunk boxes as stored
+      if (lane < count) ws.feats[q][lane] = r0;
+      if (lane + 32 < count) ws.feats[q][lane + 32] = r1;
+      if (lane < runs) ws.boxes[q][lane] = ChunkBox{{ba.x, ba.y, bb.x}, {bb.y, bc.x, bc.y}};
+    } else {
+      e = -1;
+    }
+  }
+  const bool cached = e >= 0;
+  if (!cached) e = cacheClaim(cache, slot, g, word);  // -1: build without storing
+  if (!cached) {
 #pragma unroll 1
     for (int base = 0; base < count; base += 32) {
       const int j = base + lane;
