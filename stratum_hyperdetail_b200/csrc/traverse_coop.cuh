@@ -233,13 +233,16 @@ SD Feat winnerFeature(const GroupCache& c, const float* __restrict__ W, int slot
   const LotDesc L = loadLot(W, slot);
   const int e = c.base ? usableEntry(c, __ldcg(c.dir(slot, g))) : -1;
   if (e >= 0) {
-    const int count = groupCount(L, g);
-    const uint32_t* tag = entryTag(c, uint32_t(e));
-    const float* row = W + size_t(slot) * kLotFloats;
-    bool same = true;
-#pragma unroll 1
-    for (int k = 0; k < 11 && same; k++) same = __ldg(tag + k) == tagWord(row, g, count, k);
-    if (same) return unstage(cacheRecord(c, e, i));
+    // the tag (nine descriptor words, group, count) and the record in one round trip
+    const uint4* t4 = reinterpret_cast<const uint4*>(entryTag(c, uint32_t(e)));
+    const uint4 t0 = __ldg(t4), t1 = __ldg(t4 + 1), t2 = __ldg(t4 + 2);
+    const StagedFeat rec = cacheRecord(c, e, i);
+    const uint4* r4 = reinterpret_cast<const uint4*>(W + size_t(slot) * kLotFloats);
+    const uint4 w0 = __ldg(r4), w1 = __ldg(r4 + 1), w2 = __ldg(r4 + 2);
+    const bool same = t0.x == w0.x && t0.y == w0.y && t0.z == w0.z && t0.w == w0.w && t1.x == w1.x &&
+                      t1.y == w1.y && t1.z == w1.z && t1.w == w1.w && t2.x == w2.x &&
+                      t2.y == uint32_t(g) && t2.z == uint32_t(groupCount(L, g));
+    if (same) return unstage(rec);
   }
   return featureAtOOL(L, g, i);
 }
