@@ -146,8 +146,8 @@ SD void retire(uint32_t* next, uint32_t* done, int threads) {
 }
 
 // STRATUM_TRACE_OCC / THREADS resident blocks (rounded down).  512 threads per
-// SM (128 registers, no spills): the six-view 1600x900 trace in 7.9 ms against
-// 8.3 ms at 640 (96 registers, 88/136 bytes of spills), every pose faster;
+// SM (128 registers, a few bytes of spills): the six-view 1600x900 trace 4-5 %
+// faster than at 640 (96 registers, 88/136 bytes of spills), every pose faster;
 // 768 (80 registers, heavy spills) is slower still.
 // The warp-cooperative traversal (traverse_coop.cuh) unless built with
 // STRATUM_BATCH_PER_LANE (each lane walks its own ray, as the drop-in kernel).
