@@ -200,8 +200,11 @@ unsigned long long stratum_groupCacheBytes(int entries);
 int stratum_groupCacheInit(unsigned* Groups, int entries, stratum_stream_t stream);
 
 /* Tunables of the batched trace: block size (64/128/256), tiles a warp claims
- * per queue access (queue depth, 1..16), tile order within a view (0 row-major,
- * 1 Morton-ordered 4x4-tile super-tiles).  Chosen by stratum_autotune. */
+ * per queue access (queue depth, 1..16), tile order within a view (bit 0 of
+ * order: 0 row-major, 1 Morton-ordered 4x4-tile super-tiles).  Bit 1 of order
+ * selects the block-pooled trace, in which the warps of a block serve one
+ * another's groups (same results; slower on the benchmark views, so
+ * stratum_autotune never chooses it).  Chosen by stratum_autotune. */
 typedef struct stratum_tune {
   int threads;
   int grab;

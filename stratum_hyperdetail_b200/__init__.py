@@ -91,7 +91,8 @@ SIGNATURES: dict[str, list] = {
 
 
 class Tune(ct.Structure):
-    """stratum_tune: block size, tiles per queue claim, tile order."""
+    """stratum_tune: block size, tiles per queue claim, tile order (bit 0) and
+    the block-pooled trace (bit 1 of order)."""
     _fields_ = [("threads", ct.c_int), ("grab", ct.c_int), ("order", ct.c_int)]
 
 

@@ -34,6 +34,7 @@
 #include "common_api.cuh"
 #include "hierarchy.cuh"
 #include "traverse_coop.cuh"
+#include "traverse_pool.cuh"
 #include "world.cuh"
 
 static_assert(sizeof(stratum_view) == 128, "stratum_view layout is part of the ABI");
@@ -192,6 +193,45 @@ __global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
   retire(&S->counters[kTraceNext], &S->counters[kTraceDone], THREADS);
 }
 
+// The block-pooled trace (traverse_pool.cuh): a block claims THREADS / 32
+// tiles at once, one per warp, and its warps serve one another's groups.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS, STRATUM_TRACE_OCC / THREADS)
+    tracePooledK(const stratum_view* __restrict__ V, int n, int order, BatchScratch* S) {
+  constexpr int P = THREADS / 32;
+  extern __shared__ __align__(16) unsigned char poolBytes[];
+  PoolShared<P>& sh = *reinterpret_cast<PoolShared<P>*>(poolBytes);
+  __shared__ int firstTile;
+  const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5);
+  const int total = int(S->counters[kTotalTiles]);
+#pragma unroll 1
+  for (;;) {
+    if (threadIdx.x == 0) firstTile = int(atomicAdd(&S->counters[kTraceNext], uint32_t(P)));
+    __syncthreads();
+    const int t0 = firstTile;
+    __syncthreads();  // every thread has read it before it is written again
+    if (t0 >= total) break;
+    const int tile = t0 + warp;
+    int v = 0, W = 1, H = 1, tx = 0, ty = 0;
+    bool ok = tile < total;
+    if (ok) {
+      v = viewOf(V, n, tile);
+      W = V[v].width;
+      H = V[v].height;
+      ok = tileCoord(tile - V[v].tileBase, V[v].tilesX, (H + kTileH - 1) / kTileH, order, tx, ty);
+    }
+    const int x = tx * kTileW + (lane & 7), y = ty * kTileH + (lane >> 3);
+    const bool inFrame = ok && x < W && y < H;
+    const Camera cam = S->view[v].cam;
+    const uint32_t o0 = S->view[v].o[0], o2 = S->view[v].o[2];
+    const f3 rd = primaryDir(cam, inFrame ? x : 0, inFrame ? y : 0, W, H);
+    const TraceResult r = tracePooled<P>(sh, V, v, V[v].World, reinterpret_cast<const float4*>(V[v].Nodes), o0, o2,
+                                         cam.pos, rd, 1.08f / float(H), inFrame);
+    if (inFrame) storeTrace(V[v].Hit, V[v].Surface, size_t(y) * W + x, r);
+  }
+  retire(&S->counters[kTraceNext], &S->counters[kTraceDone], THREADS);
+}
+
 // STRATUM_SHADE_OCC / THREADS resident blocks: 1536 threads per SM (40 registers,
 // some spills) measured fastest; shading is latency-bound.
 #ifndef STRATUM_SHADE_OCC
@@ -322,7 +362,7 @@ enum Parts { kTrace = 1, kShade = 2 };
 // std::call_once, so concurrent first calls (the render server's scheduler and
 // a direct caller) all see the four grids complete.
 constexpr int kGridDevices = 64;
-struct PersistentGrids { int trace, shade, light, resolve; };
+struct PersistentGrids { int trace, pooled, shade, light, resolve; };
 
 template <int T>
 int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratch* S, cudaStream_t s, int parts) {
@@ -335,22 +375,27 @@ int launchParts(const stratum_view* V, int n, const stratum_tune& t, BatchScratc
   std::call_once(once[dev], [&] {
     PersistentGrids g;
     g.trace = residentBlocks(traceViewsK<T>, T, traceSmem(T));
+    g.pooled = residentBlocks(tracePooledK<T>, T, sizeof(PoolShared<T / 32>));
     g.shade = residentBlocks(shadeViewsK<T>, T);
     g.light = residentBlocks(lightViewsK<T>, T);
     g.resolve = residentBlocks(resolveViewsK<T>, T);
     grids[dev] = g;
   });
   const PersistentGrids& g = grids[dev];
-  if (parts & kTrace) traceViewsK<T><<<g.trace, T, traceSmem(T), s>>>(V, n, t.grab, t.order, S);
-  if (parts & kShade) shadeViewsK<T><<<g.shade, T, 0, s>>>(V, n, t.grab, t.order, S);
-  if (parts & kShade) lightViewsK<T><<<g.light, T, 0, s>>>(V, n, t.grab, t.order, S);
-  if (parts & kShade) resolveViewsK<T><<<g.resolve, T, 0, s>>>(V, n, t.grab, t.order, S);
+  const int order = t.order & 1;  // tile order; bit 1 selects the block-pooled trace
+  if ((parts & kTrace) && (t.order & 2))
+    tracePooledK<T><<<g.pooled, T, sizeof(PoolShared<T / 32>), s>>>(V, n, order, S);
+  else if (parts & kTrace)
+    traceViewsK<T><<<g.trace, T, traceSmem(T), s>>>(V, n, t.grab, order, S);
+  if (parts & kShade) shadeViewsK<T><<<g.shade, T, 0, s>>>(V, n, t.grab, order, S);
+  if (parts & kShade) lightViewsK<T><<<g.light, T, 0, s>>>(V, n, t.grab, order, S);
+  if (parts & kShade) resolveViewsK<T><<<g.resolve, T, 0, s>>>(V, n, t.grab, order, S);
   return launchStatus();
 }
 
 bool tuneOk(const stratum_tune& t) {
   return (t.threads == 64 || t.threads == 128 || t.threads == 256) && t.grab >= 1 && t.grab <= 16 &&
-         (t.order == 0 || t.order == 1);
+         t.order >= 0 && t.order <= 3;
 }
 
 // parts: kTrace (with the prologue), kShade (uses the prologue's scratch), or both.
@@ -361,7 +406,7 @@ int render(stratum_view* V, int n, void* scratch, unsigned long long bytes, cons
   if (!tuneOk(t)) return STRATUM_EINVAL;
   BatchScratch* S = static_cast<BatchScratch*>(scratch);
   if (parts & kTrace) {
-    prologueK<<<1, 256, 0, s>>>(V, n, t.order, S);
+    prologueK<<<1, 256, 0, s>>>(V, n, t.order & 1, S);
     cacheResetK<<<dim3(64, n), 256, 0, s>>>(V, n);
   }
   if (t.threads == 64) return launchParts<64>(V, n, t, S, s, parts);

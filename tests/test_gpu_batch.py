@@ -48,7 +48,7 @@ def plain_frames(frames):
     return out
 
 
-@pytest.mark.parametrize("tune", [(128, 1, 1), (64, 2, 0), (256, 4, 1), (128, 16, 0)])
+@pytest.mark.parametrize("tune", [(128, 1, 1), (64, 2, 0), (256, 4, 1), (128, 16, 0), (64, 1, 3), (128, 1, 2), (256, 1, 3)])
 def test_batch_equals_plain(cuda, tune):
     from stratum_hyperdetail_b200.batch import Batch
     want = plain_frames(2)
