@@ -55,6 +55,12 @@ def test_bad_arguments_are_rejected_before_launch():
     assert L.stratum_reduceGroupBounds(ct.c_void_p(16), ct.c_void_p(16), 3, 0, None) == sb.EINVAL
     assert L.stratum_resolveFrame(None, None, None, None, None, None, -1, 5, None) == sb.EINVAL
     assert L.stratum_enumerateGroups(None, None, 1, 65, None, None, None) == sb.EINVAL
+    # tunes outside the accepted set (block size 64/128/256, queue depth 1..16,
+    # order 0..3: tile order in bit 0, the block-pooled trace in bit 1)
+    fake = ct.c_void_p(256)
+    for bad in ((128, 1, 4), (96, 1, 0), (128, 0, 0), (128, 17, 1), (64, 1, -1)):
+        t = sb.Tune(*bad)
+        assert L.stratum_renderViews(fake, 1, fake, 1 << 30, ct.byref(t), None) == sb.EINVAL, bad
 
 
 def test_abi_constants_match_reference():
